@@ -1,0 +1,392 @@
+"""Benchmark: BLS12-446 G1 MSM points/s on B200 (one JSON line on rank 0).
+
+Workload (the plain single-GPU configuration): one G1 MSM of n = 2^20
+points per GPU, scalars uniform in [0, r) with 1% zeros and 1% ones, bases
+P_i = t_i * G with 2% duplicated, 5 x u64 limbs per scalar, seeded synthetic
+data (no dataset).  With N GPUs each rank runs the same shape on its own
+shard (weak scaling); the shards' partial sums are exchanged with one
+all_gather and added on the device, as a sharded MSM does.
+
+Keys beyond the driver contract:
+  roofline      the dominant kernel (bucket accumulation) against the
+                measured IMAD peak of this GPU (bound "imad": the path is
+                exact integer arithmetic; neither tensor cores nor HBM bound it)
+  msm_roofline  the whole MSM against the same peak, with the fixed op count
+  cpu_baseline  the reference's own host code (oracle/_ref) on the host cores
+  extra         Fp 2^26 and G2 2^18 measurements, phase breakdown
+
+--impl reference times the reference's CPU implementation of the path
+(oracle/_ref, all host threads) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+LOG2N = 20
+G2_LOG2N = 18
+CPU_SAMPLE = 1 << 14
+FP_MICRO = 1 << 26
+METRIC = "MSM points/s (G1 2^20, G2 2^18) batched vs plain on 1 B200, bit-exact; p99 ms"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-extra", action="store_true", help="skip the Fp / G2 / CPU side measurements")
+    return ap.parse_args()
+
+
+def host_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: reference host code (or the oracle port) on a bounded sample
+# ---------------------------------------------------------------------------
+def cpu_baseline_run(points, scalars, threads):
+    import oracle
+    t0 = time.perf_counter()
+    res = oracle.ref_msm_pippenger(points, scalars, group=1, threads=threads)
+    kind = "reference"
+    if res is None:
+        oracle.msm_pippenger(points, scalars, group=1, threads=threads)
+        kind = "port"
+    dt = time.perf_counter() - t0
+    return len(points) / dt, kind, dt
+
+
+def cpu_sample_inputs(n):
+    """First n points of the benchmark workload, computed on the CPU."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    import oracle
+    from gpu_msm_b200 import workload as wl
+    sc = wl.make_scalars(1 << LOG2N, seed=42)[:n]
+    logs = wl.make_base_logs(1 << LOG2N, seed=4242)[:n]
+    g = oracle.g1_generator()
+    ts = wl.limbs_to_ints(logs)
+    with ThreadPoolExecutor(max_workers=host_threads()) as ex:
+        pts = list(ex.map(lambda t: oracle.scalar_mul(g, t), ts))
+    return np.concatenate(pts), sc
+
+
+def run_reference(args, rank, world):
+    """--impl reference: rank 0 times the reference CPU path; others exit."""
+    if rank != 0:
+        return
+    threads = host_threads()
+    pts, sc = cpu_sample_inputs(CPU_SAMPLE)
+    for _ in range(max(0, args.warmup)):
+        cpu_baseline_run(pts[:1024], sc[:1024], threads)
+    times, kind = [], "reference"
+    for _ in range(args.steps):
+        _, kind, dt = cpu_baseline_run(pts, sc, threads)
+        times.append(dt)
+    t = statistics.mean(times)
+    value = CPU_SAMPLE / t
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64 limbs (exact integer)", "data": "synthetic",
+        "config": {"workload": f"G1 MSM, 2^{LOG2N}-point workload, timed on its first {CPU_SAMPLE} points",
+                   "scalar_limbs": 5, "parallelism": "host threads"},
+        "cpu_baseline": {"value": value, "unit": "points/s", "cores": threads, "kind": kind,
+                         "sample": f"first {CPU_SAMPLE} points of the G1 2^{LOG2N} workload per step; "
+                                   "4-bit windows, projective buckets, combine_buckets_cpu_projective_g1"},
+        "e2e": {"value": value, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+
+    import gpu_msm_b200 as gm
+    from gpu_msm_b200 import workload as wl
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    n = 1 << LOG2N
+
+    # inputs of this rank's shard, resident in HBM before timing
+    sc = wl.make_scalars(n, seed=42 + 1000 * rank)
+    logs = wl.make_base_logs(n, seed=4242 + 1000 * rank)
+    sc_d = torch.from_numpy(sc.view(np.int64)).to(dev)
+    pts_d = gm.generator_mul_batch(torch.from_numpy(logs.view(np.int64)).to(dev), group=1)
+    torch.cuda.synchronize()
+    c = gm.default_window(1, n, 5)
+    entries = int(wl.signed_digit_counts(sc, c).sum())
+
+    gathered = torch.empty((world, gm.G1P_WORDS), dtype=torch.int64, device=dev) if world > 1 else None
+
+    def step(out):
+        gm.msm_device(pts_d, sc_d, group=1, out=out)
+        if world > 1:
+            dist.all_gather_into_tensor(gathered, out)
+            gm.sum_projective(gathered, group=1, out=out)
+
+    out = torch.empty(gm.G1P_WORDS, dtype=torch.int64, device=dev)
+    for _ in range(args.warmup):
+        step(out)
+    torch.cuda.synchronize()
+
+    # timed region: device events on the launching (current) stream
+    gm.launch_count_reset()
+    gm.profile_enable(True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        ev0.record()
+        for _ in range(args.steps):
+            step(out)
+        ev1.record()
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    launches = gm.launch_count_reset()
+    phases = gm.profile_collect()
+    gm.profile_enable(False)
+    ms = ev0.elapsed_time(ev1) / args.steps
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * n / (ms_max / 1e3)
+
+    # per-phase averages and the dominant kernel
+    acc = {}
+    for name, v in phases:
+        if name == "start":
+            continue
+        acc.setdefault(name, []).append(v)
+    phase_ms = {k: statistics.mean(v) for k, v in acc.items()}
+
+    if rank != 0:
+        return
+
+    # IMAD peak of this GPU (project microbenchmark)
+    sink = torch.empty(148 * 8 * 256 * 4, dtype=torch.int32, device=dev)
+    iters = 4096
+    gm.imad_probe(64, sink)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    best = 0.0
+    for _ in range(3):
+        e0.record()
+        cnt = gm.imad_probe(iters, sink)
+        e1.record()
+        torch.cuda.synchronize()
+        best = max(best, cnt / (e0.elapsed_time(e1) / 1e3))
+    imad_peak = best  # IMAD/s
+
+    acc_ms = phase_ms.get("accumulate", float("nan"))
+    acc_imad = 798.0 * 10 * entries
+    achieved = acc_imad / (acc_ms / 1e3)
+    msm_ops = wl.msm_roofline_imad(n, 1)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32 limbs (exact integer)", "data": "synthetic",
+        "config": {"workload": f"plain single G1 MSM, n=2^{LOG2N} per GPU, scalars < r (5 x u64), "
+                               "1% zeros, 1% ones, bases t_i*G with 2% duplicates",
+                   "window_bits": c, "entries": entries, "parallelism": f"points sharded x{world}",
+                   "l2": "inputs 168 MB > 126 MB L2 (no flush)"},
+        "roofline": {"bound": "imad", "kernel": "k_accumulate<Fp>", "achieved": achieved / 1e12,
+                     "peak": imad_peak / 1e12, "unit": "TIMAD/s", "frac": achieved / imad_peak,
+                     "traffic": None,
+                     "work": f"798 IMAD x 10 Fp mults x {entries} entries per launch",
+                     "peak_source": "measured: gm_imad_probe (independent mad.lo/mad.hi chains)"},
+        "msm_roofline": {"ops_imad": msm_ops, "achieved": msm_ops / (ms / 1e3) / 1e12,
+                         "frac": msm_ops / (ms / 1e3) / imad_peak, "unit": "TIMAD/s"},
+        "phases_ms": phase_ms,
+        "gpu_launches": int(launches),
+    }
+    line["clocks"] = clk.summary()
+
+    if world == 1:
+        line["e2e"] = measure_e2e(args, gm, sc, pts_d)
+        if not args.no_extra:
+            line["extra"] = measure_extra(gm, wl, dev, imad_peak)
+            pts_h = gm.to_numpy_points(pts_d[:CPU_SAMPLE], 1)
+            v, kind, dt = cpu_baseline_run(pts_h, sc[:CPU_SAMPLE], host_threads())
+            line["cpu_baseline"] = {
+                "value": v, "unit": "points/s", "cores": host_threads(), "kind": kind,
+                "sample": f"first {CPU_SAMPLE} points of this workload ({dt:.1f} s), reference-structured "
+                          "Pippenger: 4-bit windows, projective buckets, combine per window"}
+    print(json.dumps(line), flush=True)
+
+
+def measure_e2e(args, gm, sc, pts_d):
+    """Public host API (g1_msm_limbs_wrapper) with pinned host buffers: H2D of
+    points and scalars, the MSM and the D2H of the result in every step."""
+    import torch
+    n = len(sc)
+    pts_pin = torch.empty((n, gm.G1_WORDS), dtype=torch.int64, pin_memory=True)
+    pts_pin.copy_(pts_d.cpu())
+    sc_pin = torch.empty((n, 5), dtype=torch.int64, pin_memory=True)
+    sc_pin.copy_(torch.from_numpy(sc.view(np.int64)))
+    pts_np = pts_pin.numpy().view(np.uint64).view(gm.G1).reshape(-1)
+    sc_np = sc_pin.numpy().view(np.uint64)
+    for _ in range(2):
+        gm.msm(pts_np, sc_np, group=1, montgomery=True)
+    steps = max(3, args.steps // 2)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        gm.msm(pts_np, sc_np, group=1, montgomery=True)
+    dt = (time.perf_counter() - t0) / steps
+    return {"value": n / dt, "unit": "points/s", "h2d_bytes_per_step": n * (120 + 40),
+            "d2h_bytes_per_step": 168 + 4, "ms_per_step": dt * 1e3,
+            "api": "g1_msm_limbs_wrapper (host buffers, pinned)"}
+
+
+def measure_extra(gm, wl, dev, imad_peak):
+    import torch
+    out = {}
+    # Fp microbench: 2^26 independent fp_mont_mul pairs, Montgomery form
+    rng = np.random.default_rng(26)
+    a = torch.from_numpy(rng.integers(0, 2 ** 63, size=(FP_MICRO, 7), dtype=np.int64)).to(dev)
+    a[:, 6] &= 0x1FFFFFFFFFFFFFFF
+    b = torch.roll(a, 1, 0)
+    c = torch.empty_like(a)
+    for _ in range(2):
+        gm.field_mul_array(a, b, op="fp_mont_mul", out=c)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    reps = 5
+    for _ in range(reps):
+        gm.field_mul_array(a, b, op="fp_mont_mul", out=c)
+    e1.record()
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / reps / 1e3
+    out["fp_mont_mul_2^26"] = {"muls_per_s": FP_MICRO / t, "ms": t * 1e3,
+                               "imad_frac": FP_MICRO * 798 / t / imad_peak,
+                               "hbm_gbs": FP_MICRO * 168 / t / 1e9}
+    del a, b, c
+    # G2 2^18
+    n2 = 1 << G2_LOG2N
+    sc2 = wl.make_scalars(n2, seed=43, one_frac=0.0)
+    logs2 = wl.make_base_logs(n2, seed=4343)
+    sc2_d = torch.from_numpy(sc2.view(np.int64)).to(dev)
+    pts2 = gm.generator_mul_batch(torch.from_numpy(logs2.view(np.int64)).to(dev), group=2)
+    o2 = torch.empty(gm.G2P_WORDS, dtype=torch.int64, device=dev)
+    gm.msm_device(pts2, sc2_d, group=2, out=o2)
+    torch.cuda.synchronize()
+    e0.record()
+    reps = 3
+    for _ in range(reps):
+        gm.msm_device(pts2, sc2_d, group=2, out=o2)
+    e1.record()
+    torch.cuda.synchronize()
+    t2 = e0.elapsed_time(e1) / reps / 1e3
+    ops2 = wl.msm_roofline_imad(n2, 2)
+    out["g2_msm_2^18"] = {"points_per_s": n2 / t2, "ms": t2 * 1e3, "imad_frac": ops2 / t2 / imad_peak,
+                          "window_bits": gm.default_window(2, n2, 5)}
+    return out
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

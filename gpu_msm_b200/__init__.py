@@ -1,0 +1,350 @@
+"""gpu_msm_b200 -- B200-native (sm_100a) BLS12-446 multi-scalar multiplication.
+
+Python host mirror of the library's C-ABI (``include/gpu_msm_b200.h``).  The
+compute path is the CUDA shared library ``libgpu_msm_b200.so`` built in-tree
+by ``gpu_msm_b200/Makefile``; this module only loads it with ``ctypes`` and
+moves buffers.  There is no CPU fallback: if the library is missing every
+call raises.
+
+Function names follow the reference's C-ABI and C++ API
+(pdroalves/gpu_msm rust-api/include/rust_wrapper.h, include/curve.h):
+
+* ``g1_msm_wrapper`` / ``g2_msm_wrapper`` -- host buffers, u64 scalars, same
+  Montgomery conventions as the reference wrappers (G1 points in standard
+  form, G2 points in Montgomery form);
+* ``g1_msm`` / ``g2_msm`` -- host buffers, multi-limb scalars;
+* ``msm_device`` -- device tensors, asynchronous on the current torch stream
+  (the ``point_msm_async`` / ``point_msm_u64_async_g1`` analogue);
+* ``projective_to_affine`` / ``affine_to_projective`` / ``from_montgomery`` ...
+  the host-side point helpers of the reference's C wrapper.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libgpu_msm_b200.so")
+
+# numpy dtypes byte-compatible with the C structs (include/gpu_msm_b200.h)
+FP = np.dtype(("<u8", (7,)))
+FP2 = np.dtype(("<u8", (2, 7)))
+G1 = np.dtype([("x", "<u8", (7,)), ("y", "<u8", (7,)), ("infinity", "u1"), ("_pad", "u1", (7,))])
+G2 = np.dtype([("x", "<u8", (2, 7)), ("y", "<u8", (2, 7)), ("infinity", "u1"), ("_pad", "u1", (7,))])
+G1P = np.dtype([("X", "<u8", (7,)), ("Y", "<u8", (7,)), ("Z", "<u8", (7,))])
+G2P = np.dtype([("X", "<u8", (2, 7)), ("Y", "<u8", (2, 7)), ("Z", "<u8", (2, 7))])
+
+# u64 words per struct, for torch int64 views of device buffers
+G1_WORDS, G2_WORDS, G1P_WORDS, G2P_WORDS = 15, 29, 21, 42
+
+STATUS = {0: "ok", -1: "bad size or argument", -2: "stream creation failed", -3: "allocation failed",
+          -4: "CUDA error", -5: "device consistency check failed"}
+
+C_API = [
+    # reference C-ABI (rust_wrapper.h)
+    "affine_to_projective_g1_wrapper", "affine_to_projective_g2_wrapper",
+    "projective_to_affine_g1_wrapper", "projective_to_affine_g2_wrapper",
+    "g1_point_at_infinity_wrapper", "g2_point_at_infinity_wrapper",
+    "g1_projective_point_at_infinity_wrapper", "g2_projective_point_at_infinity_wrapper",
+    "g1_is_infinity_wrapper", "g2_is_infinity_wrapper", "g1_msm_wrapper", "g2_msm_wrapper",
+    "g1_from_montgomery_wrapper", "g2_from_montgomery_wrapper", "fp_to_montgomery_wrapper",
+    "init_device_generators",
+    # additive entry points
+    "g1_msm_limbs_wrapper", "g2_msm_limbs_wrapper", "gm_g1_msm_device", "gm_g2_msm_device",
+    "gm_g1_msm_device_c", "gm_g2_msm_device_c", "gm_msm_default_window",
+    "gm_fp_mont_mul_array", "gm_fp_mul_array", "gm_fp2_mont_mul_array", "gm_fp2_mul_array",
+    "gm_g1_to_montgomery_batch", "gm_g2_to_montgomery_batch",
+    "gm_g1_generator_mul_batch", "gm_g2_generator_mul_batch", "gm_last_error",
+    "gm_profile_enable", "gm_profile_collect", "gm_launch_count_reset", "gm_imad_probe",
+    "gm_g1_sum_projective", "gm_g2_sum_projective",
+]
+
+
+class MSMError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load libgpu_msm_b200.so; raises if it was not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise MSMError(f"CUDA library not built: {LIB_PATH} (run `make -C gpu_msm_b200`)")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, i32, u32, i64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_uint32, ctypes.c_int64
+        for name in ("g1_msm_wrapper", "g2_msm_wrapper"):
+            getattr(L, name).argtypes = [vp, vp, vp, i32, u32]
+        for name in ("g1_msm_limbs_wrapper", "g2_msm_limbs_wrapper"):
+            getattr(L, name).argtypes = [vp, vp, vp, i32, i32, u32, i32]
+        for name in ("gm_g1_msm_device", "gm_g2_msm_device"):
+            getattr(L, name).argtypes = [vp, u32, vp, vp, vp, i32, i32]
+        for name in ("gm_g1_msm_device_c", "gm_g2_msm_device_c"):
+            getattr(L, name).argtypes = [vp, u32, vp, vp, vp, i32, i32, i32]
+        L.gm_msm_default_window.argtypes = [i32, i64, i32]
+        for name in ("gm_fp_mont_mul_array", "gm_fp_mul_array", "gm_fp2_mont_mul_array", "gm_fp2_mul_array"):
+            getattr(L, name).argtypes = [vp, u32, vp, vp, vp, i64]
+        for name in ("gm_g1_to_montgomery_batch", "gm_g2_to_montgomery_batch"):
+            getattr(L, name).argtypes = [vp, u32, vp, i32]
+        for name in ("gm_g1_generator_mul_batch", "gm_g2_generator_mul_batch"):
+            getattr(L, name).argtypes = [vp, u32, vp, vp, i32, i32]
+        L.gm_last_error.restype = ctypes.c_char_p
+        for name in ("g1_is_infinity_wrapper", "g2_is_infinity_wrapper"):
+            getattr(L, name).restype = ctypes.c_bool
+        L.init_device_generators.argtypes = [vp, u32]
+        L.gm_profile_enable.argtypes = [i32]
+        L.gm_profile_collect.argtypes = [ctypes.c_char_p, i32, vp, i32]
+        L.gm_launch_count_reset.restype = i64
+        L.gm_imad_probe.argtypes = [vp, u32, i32, vp, i64, vp]
+        for name in ("gm_g1_sum_projective", "gm_g2_sum_projective"):
+            getattr(L, name).argtypes = [vp, u32, vp, vp, i32]
+        _lib = L
+    return _lib
+
+
+def _check(rc: int, what: str):
+    if rc != 0:
+        msg = lib().gm_last_error().decode(errors="replace")
+        raise MSMError(f"{what} failed: {rc} ({STATUS.get(rc, '?')}) {msg}")
+
+
+def _p(a: np.ndarray):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def _grp(group: int):
+    if group == 1:
+        return G1, G1P, "g1"
+    if group == 2:
+        return G2, G2P, "g2"
+    raise ValueError("group must be 1 or 2")
+
+
+def _scalars_2d(scalars, n: int) -> np.ndarray:
+    s = np.ascontiguousarray(scalars, dtype=np.uint64)
+    if s.ndim == 1:
+        s = s.reshape(n, -1) if n else s.reshape(0, 1)
+    if s.shape[0] != n:
+        raise ValueError("scalars must have one row per point")
+    return s
+
+
+# ---------------------------------------------------------------------------
+# host-buffer MSM
+# ---------------------------------------------------------------------------
+
+def g1_msm_wrapper(points: np.ndarray, scalars: np.ndarray, gpu_index: int = 0) -> np.ndarray:
+    """Reference ``g1_msm_wrapper``: standard-form G1 points, u64 scalars."""
+    pts = np.ascontiguousarray(points, dtype=G1)
+    sc = np.ascontiguousarray(scalars, dtype=np.uint64).reshape(-1)
+    out = np.zeros(1, dtype=G1P)
+    _check(lib().g1_msm_wrapper(_p(out), _p(pts), _p(sc), len(pts), gpu_index), "g1_msm_wrapper")
+    return out
+
+
+def g2_msm_wrapper(points: np.ndarray, scalars: np.ndarray, gpu_index: int = 0) -> np.ndarray:
+    """Reference ``g2_msm_wrapper``: Montgomery-form G2 points, u64 scalars."""
+    pts = np.ascontiguousarray(points, dtype=G2)
+    sc = np.ascontiguousarray(scalars, dtype=np.uint64).reshape(-1)
+    out = np.zeros(1, dtype=G2P)
+    _check(lib().g2_msm_wrapper(_p(out), _p(pts), _p(sc), len(pts), gpu_index), "g2_msm_wrapper")
+    return out
+
+
+def msm(points: np.ndarray, scalars: np.ndarray, group: int = 1, montgomery: bool = True,
+        gpu_index: int = 0) -> np.ndarray:
+    """sum_i scalars[i] * points[i] for host buffers; scalars are (n, limbs)
+    little-endian u64.  Returns a projective point (Montgomery form)."""
+    adt, pdt, g = _grp(group)
+    pts = np.ascontiguousarray(points, dtype=adt)
+    sc = _scalars_2d(scalars, len(pts))
+    out = np.zeros(1, dtype=pdt)
+    fn = getattr(lib(), f"{g}_msm_limbs_wrapper")
+    _check(fn(_p(out), _p(pts), _p(sc), sc.shape[1], len(pts), gpu_index, 1 if montgomery else 0),
+           f"{g}_msm_limbs_wrapper")
+    return out
+
+
+def g1_msm(points, scalars, montgomery=True, gpu_index=0):
+    return msm(points, scalars, 1, montgomery, gpu_index)
+
+
+def g2_msm(points, scalars, montgomery=True, gpu_index=0):
+    return msm(points, scalars, 2, montgomery, gpu_index)
+
+
+def default_window(group: int, n: int, scalar_limbs: int) -> int:
+    return int(lib().gm_msm_default_window(group, n, scalar_limbs))
+
+
+# ---------------------------------------------------------------------------
+# host point helpers (reference c_wrapper.cu)
+# ---------------------------------------------------------------------------
+
+def projective_to_affine(proj: np.ndarray, group: int = 1) -> np.ndarray:
+    adt, pdt, g = _grp(group)
+    p = np.ascontiguousarray(proj, dtype=pdt).reshape(-1)
+    out = np.zeros(len(p), dtype=adt)
+    fn = getattr(lib(), f"projective_to_affine_{g}_wrapper")
+    for i in range(len(p)):
+        fn(ctypes.c_void_p(out.ctypes.data + i * adt.itemsize), ctypes.c_void_p(p.ctypes.data + i * pdt.itemsize))
+    return out
+
+
+def affine_to_projective(aff: np.ndarray, group: int = 1) -> np.ndarray:
+    adt, pdt, g = _grp(group)
+    a = np.ascontiguousarray(aff, dtype=adt).reshape(-1)
+    out = np.zeros(len(a), dtype=pdt)
+    fn = getattr(lib(), f"affine_to_projective_{g}_wrapper")
+    for i in range(len(a)):
+        fn(ctypes.c_void_p(out.ctypes.data + i * pdt.itemsize), ctypes.c_void_p(a.ctypes.data + i * adt.itemsize))
+    return out
+
+
+def from_montgomery(aff: np.ndarray, group: int = 1) -> np.ndarray:
+    adt, _, g = _grp(group)
+    a = np.ascontiguousarray(aff, dtype=adt).reshape(-1)
+    out = np.zeros(len(a), dtype=adt)
+    fn = getattr(lib(), f"{g}_from_montgomery_wrapper")
+    for i in range(len(a)):
+        fn(ctypes.c_void_p(out.ctypes.data + i * adt.itemsize), ctypes.c_void_p(a.ctypes.data + i * adt.itemsize))
+    return out
+
+
+def fp_to_montgomery(vals: np.ndarray) -> np.ndarray:
+    v = np.ascontiguousarray(vals, dtype=np.uint64).reshape(-1, 7)
+    out = np.zeros_like(v)
+    for i in range(len(v)):
+        lib().fp_to_montgomery_wrapper(ctypes.c_void_p(out.ctypes.data + 56 * i), ctypes.c_void_p(v.ctypes.data + 56 * i))
+    return out
+
+
+def canonical_affine(proj: np.ndarray, group: int = 1) -> np.ndarray:
+    """Projective (Montgomery) -> affine in standard form, the representation
+    results are compared in."""
+    return from_montgomery(projective_to_affine(proj, group), group)
+
+
+# ---------------------------------------------------------------------------
+# device-resident API (torch tensors as buffers, current torch stream)
+# ---------------------------------------------------------------------------
+
+def _stream_handle(stream=None):
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+def _dev_index(t) -> int:
+    return t.device.index if t.device.index is not None else 0
+
+
+def msm_device(points, scalars, group: int = 1, window_bits: int = 0, out=None, stream=None):
+    """Asynchronous MSM on device tensors.
+
+    points:  int64 tensor (n, 15) [G1Point] or (n, 29) [G2Point], Montgomery form
+    scalars: int64 tensor (n, limbs), little-endian u64 limbs
+    returns: int64 tensor (21,) or (42,) -- projective result, Montgomery form
+    """
+    import torch
+    n = points.shape[0]
+    limbs = scalars.shape[1] if scalars.dim() == 2 else 1
+    words = G1P_WORDS if group == 1 else G2P_WORDS
+    if out is None:
+        out = torch.empty(words, dtype=torch.int64, device=points.device)
+    fn = lib().gm_g1_msm_device_c if group == 1 else lib().gm_g2_msm_device_c
+    _check(fn(_stream_handle(stream), _dev_index(points), ctypes.c_void_p(out.data_ptr()),
+              ctypes.c_void_p(points.data_ptr()), ctypes.c_void_p(scalars.data_ptr()), limbs, n, window_bits),
+           "msm_device")
+    return out
+
+
+def sum_projective(points, group: int = 1, out=None, stream=None):
+    """Device sum of projective points (int64 tensor (k, 21) or (k, 42))."""
+    import torch
+    words = G1P_WORDS if group == 1 else G2P_WORDS
+    if out is None:
+        out = torch.empty(words, dtype=torch.int64, device=points.device)
+    fn = lib().gm_g1_sum_projective if group == 1 else lib().gm_g2_sum_projective
+    _check(fn(_stream_handle(stream), _dev_index(points), ctypes.c_void_p(out.data_ptr()),
+              ctypes.c_void_p(points.data_ptr()), points.shape[0]), "sum_projective")
+    return out
+
+
+def generator_mul_batch(scalars, group: int = 1, stream=None):
+    """out[i] = scalars[i] * G (canonical Montgomery affine) on the device."""
+    import torch
+    n = scalars.shape[0]
+    limbs = scalars.shape[1]
+    words = G1_WORDS if group == 1 else G2_WORDS
+    out = torch.empty((n, words), dtype=torch.int64, device=scalars.device)
+    fn = lib().gm_g1_generator_mul_batch if group == 1 else lib().gm_g2_generator_mul_batch
+    _check(fn(_stream_handle(stream), _dev_index(scalars), ctypes.c_void_p(out.data_ptr()),
+              ctypes.c_void_p(scalars.data_ptr()), limbs, n), "generator_mul_batch")
+    return out
+
+
+def to_montgomery_batch(points, group: int = 1, stream=None):
+    fn = lib().gm_g1_to_montgomery_batch if group == 1 else lib().gm_g2_to_montgomery_batch
+    _check(fn(_stream_handle(stream), _dev_index(points), ctypes.c_void_p(points.data_ptr()), points.shape[0]),
+           "to_montgomery_batch")
+    return points
+
+
+def field_mul_array(a, b, op: str = "fp_mont_mul", out=None, stream=None):
+    """Element-wise field products on device tensors of shape (n, 7) [Fp] or
+    (n, 14) [Fp2], int64.  op: fp_mont_mul | fp_mul | fp2_mont_mul | fp2_mul."""
+    import torch
+    if out is None:
+        out = torch.empty_like(a)
+    fn = getattr(lib(), f"gm_{op}_array")
+    _check(fn(_stream_handle(stream), _dev_index(a), ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(a.data_ptr()),
+              ctypes.c_void_p(b.data_ptr()), a.shape[0]), op)
+    return out
+
+
+def to_numpy_points(t, group: int = 1) -> np.ndarray:
+    """Copy an int64 device/host tensor of points to a numpy structured array."""
+    arr = t.detach().cpu().numpy().view(np.uint64)
+    adt = G1 if group == 1 else G2
+    return np.ascontiguousarray(arr).view(adt).reshape(-1)
+
+
+def to_numpy_proj(t, group: int = 1) -> np.ndarray:
+    arr = t.detach().cpu().numpy().view(np.uint64)
+    pdt = G1P if group == 1 else G2P
+    return np.ascontiguousarray(arr).view(pdt).reshape(-1)
+
+
+# ---------------------------------------------------------------------------
+# measurement hooks
+# ---------------------------------------------------------------------------
+
+def profile_enable(on: bool = True):
+    lib().gm_profile_enable(1 if on else 0)
+
+
+def profile_collect(max_phases: int = 4096):
+    """[(phase, ms), ...] for the MSMs run since profiling was enabled
+    (synchronises the recorded events)."""
+    names = ctypes.create_string_buffer(64 * max_phases)
+    ms = np.zeros(max_phases, dtype=np.float32)
+    n = lib().gm_profile_collect(names, len(names), ctypes.c_void_p(ms.ctypes.data), max_phases)
+    labels = names.value.decode().split(",") if n else []
+    return list(zip(labels, ms[:n].tolist()))
+
+
+def launch_count_reset() -> int:
+    return int(lib().gm_launch_count_reset())
+
+
+def imad_probe(iters: int, sink, stream=None) -> int:
+    """Launch the IMAD throughput probe; returns IMADs per launch."""
+    cnt = ctypes.c_int64(0)
+    _check(lib().gm_imad_probe(_stream_handle(stream), _dev_index(sink), iters, ctypes.c_void_p(sink.data_ptr()),
+                               sink.numel(), ctypes.byref(cnt)), "imad_probe")
+    return cnt.value

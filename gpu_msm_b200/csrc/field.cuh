@@ -1,0 +1,395 @@
+// BLS12-446 base field Fp on sm_100a: 14 x 32-bit little-endian limbs.
+//
+// The limb layout is byte-identical to the reference's `Fp{uint64_t limb[7]}`
+// (pdroalves/gpu_msm include/fp.h:13) on a little-endian machine, so device
+// buffers cross the ABI without conversion.  Values are in Montgomery form with
+// R = 2^448 (src/fp.cu:15-33).
+//
+// Montgomery multiplication is CIOS over 32-bit limbs on the IMAD pipe with PTX
+// carry chains (mad.lo.cc / madc.hi.cc).  To keep one carry flag per chain,
+// the partial products a_j*b_i are split by the parity of j into two
+// accumulators: X holds the even-j products (aligned at word 0) and Y the odd-j
+// products (aligned at word 1).  Neither accumulator is shifted per iteration;
+// the low column i is settled by tracking its exact carry c into column i+1,
+// and the two halves are merged once at the end.  Per multiplication this is
+// 2*14*14 product IMADs + 2*14*14 reduction IMADs + 14 quotient IMADs = 798.
+//
+// Two reduction modes:
+//   * strict: inputs < p, output < p (canonical, bit-exact with the
+//     reference's fp_mont_mul, src/fp.cu:370);
+//   * lazy:   inputs < 2p, output < 2p (no final subtraction; valid because
+//     4p < R).  Used inside point arithmetic; values are canonicalised before
+//     any equality test and before leaving the device.
+#pragma once
+#include <cstdint>
+
+#define GM_DEVI __device__ __forceinline__
+#define GM_HDI __host__ __device__ __forceinline__
+
+namespace gm {
+
+constexpr int NL = 14;  // 32-bit limbs per Fp element
+
+struct fp_t {
+  uint32_t v[NL];
+};
+
+// Field constants as constexpr limb accessors: usable with compile-time
+// indices (folded to immediates) and with run-time indices in device code.
+struct FpConst {
+  // p (src/fp.cu:15)
+  GM_HDI static constexpr uint32_t P(int i) {
+    switch (i) {
+      case 0: return 0xaab0aaabu;
+      case 1: return 0x311c0026u;
+      case 2: return 0xc573b5ccu;
+      case 3: return 0x56ee4528u;
+      case 4: return 0xe23acdeeu;
+      case 5: return 0x824e6dc3u;
+      case 6: return 0xbac71602u;
+      case 7: return 0x0f75a64bu;
+      case 8: return 0x8a02fe32u;
+      case 9: return 0x0095a4b7u;
+      case 10: return 0x65aad640u;
+      case 11: return 0x200fc349u;
+      case 12: return 0x28c5e535u;
+      case 13: return 0x3cdee0fbu;
+      default: return 0u;
+    }
+  }
+  // 2p
+  GM_HDI static constexpr uint32_t P2(int i) {
+    switch (i) {
+      case 0: return 0x55615556u;
+      case 1: return 0x6238004du;
+      case 2: return 0x8ae76b98u;
+      case 3: return 0xaddc8a51u;
+      case 4: return 0xc4759bdcu;
+      case 5: return 0x049cdb87u;
+      case 6: return 0x758e2c05u;
+      case 7: return 0x1eeb4c97u;
+      case 8: return 0x1405fc64u;
+      case 9: return 0x012b496fu;
+      case 10: return 0xcb55ac80u;
+      case 11: return 0x401f8692u;
+      case 12: return 0x518bca6au;
+      case 13: return 0x79bdc1f6u;
+      default: return 0u;
+    }
+  }
+  // R^2 mod p (src/fp.cu:21)
+  GM_HDI static constexpr uint32_t R2(int i) {
+    switch (i) {
+      case 0: return 0xdc752b45u;
+      case 1: return 0x2aff01ddu;
+      case 2: return 0x421ccf5bu;
+      case 3: return 0x92c772a7u;
+      case 4: return 0xc347dad6u;
+      case 5: return 0x140eef29u;
+      case 6: return 0x22ea595eu;
+      case 7: return 0xf5a1400cu;
+      case 8: return 0xec145218u;
+      case 9: return 0x99d91c9fu;
+      case 10: return 0x90143d4bu;
+      case 11: return 0x3bb6537fu;
+      case 12: return 0x9be7974fu;
+      case 13: return 0x3627854cu;
+      default: return 0u;
+    }
+  }
+  // R mod p = 1 in Montgomery form
+  GM_HDI static constexpr uint32_t ONE(int i) {
+    switch (i) {
+      case 0: return 0x553d5554u;
+      case 1: return 0x3b8fff65u;
+      case 2: return 0xea3128cfu;
+      case 3: return 0xa446eb5cu;
+      case 4: return 0x7714c846u;
+      case 5: return 0xf6c648f0u;
+      case 6: return 0x14e3a7f5u;
+      case 7: return 0xc22966d1u;
+      case 8: return 0xd7f40737u;
+      case 9: return 0xfda96d21u;
+      case 10: return 0x6954a6ffu;
+      case 11: return 0x7fc0f2dau;
+      case 12: return 0x5ce86b2bu;
+      case 13: return 0x0c847c13u;
+      default: return 0u;
+    }
+  }
+  // -p^-1 mod 2^32
+  static constexpr uint32_t PINV = 0x0035fffdu;
+};
+
+// ---------------------------------------------------------------------------
+// PTX carry-chain primitives.  `asm volatile` keeps the chain order; ptxas
+// maps the PTX condition code onto carry predicates.
+// ---------------------------------------------------------------------------
+GM_DEVI uint32_t mad_lo_cc(uint32_t a, uint32_t b, uint32_t c) {
+  uint32_t r;
+  asm volatile("mad.lo.cc.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(c));
+  return r;
+}
+GM_DEVI uint32_t madc_lo_cc(uint32_t a, uint32_t b, uint32_t c) {
+  uint32_t r;
+  asm volatile("madc.lo.cc.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(c));
+  return r;
+}
+GM_DEVI uint32_t madc_hi_cc(uint32_t a, uint32_t b, uint32_t c) {
+  uint32_t r;
+  asm volatile("madc.hi.cc.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(c));
+  return r;
+}
+GM_DEVI uint32_t add_cc(uint32_t a, uint32_t b) {
+  uint32_t r;
+  asm volatile("add.cc.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+  return r;
+}
+GM_DEVI uint32_t addc_cc(uint32_t a, uint32_t b) {
+  uint32_t r;
+  asm volatile("addc.cc.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+  return r;
+}
+GM_DEVI uint32_t addc(uint32_t a, uint32_t b) {
+  uint32_t r;
+  asm volatile("addc.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+  return r;
+}
+GM_DEVI uint32_t sub_cc(uint32_t a, uint32_t b) {
+  uint32_t r;
+  asm volatile("sub.cc.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+  return r;
+}
+GM_DEVI uint32_t subc_cc(uint32_t a, uint32_t b) {
+  uint32_t r;
+  asm volatile("subc.cc.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+  return r;
+}
+GM_DEVI uint32_t subc(uint32_t a, uint32_t b) {
+  uint32_t r;
+  asm volatile("subc.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+  return r;
+}
+
+// ---------------------------------------------------------------------------
+// Helpers on raw limb arrays
+// ---------------------------------------------------------------------------
+
+// r = a - m for the constant m = p (TWO_P = false) or 2p; returns borrow
+template <bool TWO_P>
+GM_DEVI uint32_t sub_const(uint32_t r[NL], const uint32_t a[NL]) {
+  r[0] = sub_cc(a[0], TWO_P ? FpConst::P2(0) : FpConst::P(0));
+#pragma unroll
+  for (int i = 1; i < NL; i++) r[i] = subc_cc(a[i], TWO_P ? FpConst::P2(i) : FpConst::P(i));
+  return subc(0, 0) & 1u;
+}
+
+// if a >= m: a -= m (constant-flow select), m = p or 2p
+template <bool TWO_P>
+GM_DEVI void cond_sub(uint32_t a[NL]) {
+  uint32_t t[NL];
+  const uint32_t borrow = sub_const<TWO_P>(t, a);
+#pragma unroll
+  for (int i = 0; i < NL; i++) a[i] = borrow ? a[i] : t[i];
+}
+
+// ---------------------------------------------------------------------------
+// Montgomery multiplication (see header comment for the scheme).
+// ---------------------------------------------------------------------------
+template <bool STRICT>
+GM_DEVI void mont_mul_raw(uint32_t r[NL], const uint32_t a[NL], const uint32_t b[NL]) {
+  uint32_t X[2 * NL], Y[2 * NL];
+#pragma unroll
+  for (int k = 0; k < NL; k++) {
+    X[k] = 0;
+    Y[k] = 0;
+  }
+  uint32_t c = 0;  // exact carry out of the settled low columns
+#pragma unroll
+  for (int i = 0; i < NL; i++) {
+    const uint32_t bi = b[i];
+    // X += sum_{j even} a_j*b_i at words i+j, i+j+1
+    X[i] = mad_lo_cc(a[0], bi, X[i]);
+    X[i + 1] = madc_hi_cc(a[0], bi, X[i + 1]);
+#pragma unroll
+    for (int j = 2; j < NL; j += 2) {
+      X[i + j] = madc_lo_cc(a[j], bi, X[i + j]);
+      X[i + j + 1] = madc_hi_cc(a[j], bi, X[i + j + 1]);
+    }
+    X[i + NL] = addc(0, 0);
+    // Y += sum_{j odd} a_j*b_i at words i+j-1, i+j (Y is one word up)
+    Y[i] = mad_lo_cc(a[1], bi, Y[i]);
+    Y[i + 1] = madc_hi_cc(a[1], bi, Y[i + 1]);
+#pragma unroll
+    for (int j = 3; j < NL; j += 2) {
+      Y[i + j - 1] = madc_lo_cc(a[j], bi, Y[i + j - 1]);
+      Y[i + j] = madc_hi_cc(a[j], bi, Y[i + j]);
+    }
+    Y[i + NL] = addc(0, 0);
+
+    // quotient digit from the exact low word of column i
+    const uint32_t u = (i == 0) ? X[0] : X[i] + Y[i - 1] + c;
+    const uint32_t m = u * FpConst::PINV;
+
+    X[i] = mad_lo_cc(m, FpConst::P(0), X[i]);
+    X[i + 1] = madc_hi_cc(m, FpConst::P(0), X[i + 1]);
+#pragma unroll
+    for (int j = 2; j < NL; j += 2) {
+      X[i + j] = madc_lo_cc(m, FpConst::P(j), X[i + j]);
+      X[i + j + 1] = madc_hi_cc(m, FpConst::P(j), X[i + j + 1]);
+    }
+    X[i + NL] = addc(X[i + NL], 0);
+    Y[i] = mad_lo_cc(m, FpConst::P(1), Y[i]);
+    Y[i + 1] = madc_hi_cc(m, FpConst::P(1), Y[i + 1]);
+#pragma unroll
+    for (int j = 3; j < NL; j += 2) {
+      Y[i + j - 1] = madc_lo_cc(m, FpConst::P(j), Y[i + j - 1]);
+      Y[i + j] = madc_hi_cc(m, FpConst::P(j), Y[i + j]);
+    }
+    Y[i + NL] = addc(Y[i + NL], 0);
+
+    // column i is now 0 mod 2^32: carry its exact high part into column i+1
+    if (i == 0) {
+      c = 0;  // X[0] == 0 exactly
+    } else {
+      uint32_t t = add_cc(X[i], Y[i - 1]);
+      uint32_t c1 = addc(0, 0);
+      t = add_cc(t, c);
+      c = addc(c1, 0);
+      (void)t;
+    }
+  }
+  // result = (X[14..27] + Y[13..26] + c), Y[27] is 0 by the size bound
+  r[0] = add_cc(X[NL], Y[NL - 1]);
+#pragma unroll
+  for (int k = 1; k < NL; k++) r[k] = addc_cc(X[NL + k], Y[NL - 1 + k]);
+  r[0] = add_cc(r[0], c);
+#pragma unroll
+  for (int k = 1; k < NL; k++) r[k] = addc_cc(r[k], 0);
+  if (STRICT) cond_sub<false>(r);
+}
+
+// ---------------------------------------------------------------------------
+// Field element API
+// ---------------------------------------------------------------------------
+struct Fp {
+  using T = fp_t;
+  static constexpr int LIMBS = NL;
+
+  GM_DEVI static fp_t zero() {
+    fp_t r;
+#pragma unroll
+    for (int i = 0; i < NL; i++) r.v[i] = 0;
+    return r;
+  }
+  GM_DEVI static fp_t one() {
+    fp_t r;
+#pragma unroll
+    for (int i = 0; i < NL; i++) r.v[i] = FpConst::ONE(i);
+    return r;
+  }
+  GM_DEVI static bool is_zero_raw(const fp_t &a) {
+    uint32_t acc = 0;
+#pragma unroll
+    for (int i = 0; i < NL; i++) acc |= a.v[i];
+    return acc == 0;
+  }
+  // a < 2p: a == 0 (mod p)
+  GM_DEVI static bool is_zero(const fp_t &a) {
+    uint32_t z = 0, q = 0;
+#pragma unroll
+    for (int i = 0; i < NL; i++) {
+      z |= a.v[i];
+      q |= a.v[i] ^ FpConst::P(i);
+    }
+    return z == 0 || q == 0;
+  }
+  // strict: a, b < p -> < p
+  GM_DEVI static fp_t add(const fp_t &a, const fp_t &b) {
+    fp_t r;
+    r.v[0] = add_cc(a.v[0], b.v[0]);
+#pragma unroll
+    for (int i = 1; i < NL; i++) r.v[i] = addc_cc(a.v[i], b.v[i]);
+    cond_sub<false>(r.v);
+    return r;
+  }
+  GM_DEVI static fp_t sub(const fp_t &a, const fp_t &b) {
+    fp_t r;
+    r.v[0] = sub_cc(a.v[0], b.v[0]);
+#pragma unroll
+    for (int i = 1; i < NL; i++) r.v[i] = subc_cc(a.v[i], b.v[i]);
+    const uint32_t mask = 0u - (subc(0, 0) & 1u);
+    r.v[0] = add_cc(r.v[0], FpConst::FpConst::P(0) & mask);
+#pragma unroll
+    for (int i = 1; i < NL; i++) r.v[i] = addc_cc(r.v[i], FpConst::P(i) & mask);
+    return r;
+  }
+  GM_DEVI static fp_t dbl(const fp_t &a) { return add(a, a); }
+  GM_DEVI static fp_t neg(const fp_t &a) {
+    // p - a for a != 0, else 0 (src/fp.cu:436)
+    if (is_zero_raw(a)) return a;
+    fp_t r;
+    r.v[0] = sub_cc(FpConst::FpConst::P(0), a.v[0]);
+#pragma unroll
+    for (int i = 1; i < NL; i++) r.v[i] = subc_cc(FpConst::P(i), a.v[i]);
+    return r;
+  }
+  GM_DEVI static fp_t mul(const fp_t &a, const fp_t &b) {
+    fp_t r;
+    mont_mul_raw<true>(r.v, a.v, b.v);
+    return r;
+  }
+  GM_DEVI static fp_t sqr(const fp_t &a) { return mul(a, a); }
+  GM_DEVI static fp_t to_mont(const fp_t &a) {
+    fp_t r2;
+#pragma unroll
+    for (int i = 0; i < NL; i++) r2.v[i] = FpConst::R2(i);
+    return mul(a, r2);
+  }
+  GM_DEVI static fp_t from_mont(const fp_t &a) {
+    fp_t o = zero();
+    o.v[0] = 1;
+    return mul(a, o);
+  }
+  GM_DEVI static fp_t small(uint32_t k) {  // k in Montgomery form
+    fp_t t = zero();
+    t.v[0] = k;
+    return to_mont(t);
+  }
+  GM_DEVI static bool eq(const fp_t &a, const fp_t &b) {
+    uint32_t d = 0;
+#pragma unroll
+    for (int i = 0; i < NL; i++) d |= a.v[i] ^ b.v[i];
+    return d == 0;
+  }
+  // Montgomery-form inverse by Fermat, a^(p-2); 0 -> 0 (src/fp.cu:545).
+  // Left-to-right square-and-multiply over the fixed exponent.
+  __device__ static fp_t inv(const fp_t &a) {
+    fp_t acc = one();
+    for (int w = NL - 1; w >= 0; w--) {
+      const uint32_t e = (w == 0) ? FpConst::P(0) - 2u : FpConst::P(w);
+      for (int b = 31; b >= 0; b--) {
+        acc = sqr(acc);
+        if ((e >> b) & 1u) acc = mul(acc, a);
+      }
+    }
+    return acc;
+  }
+};
+
+// 16-byte vector loads/stores of field elements (56 B = 3.5 x 16 B, so
+// records are laid out with 16-byte alignment by the packers).
+GM_DEVI void load_fp_u64(fp_t &r, const uint64_t *src) {
+#pragma unroll
+  for (int i = 0; i < NL / 2; i++) {
+    const uint64_t w = src[i];
+    r.v[2 * i] = (uint32_t)w;
+    r.v[2 * i + 1] = (uint32_t)(w >> 32);
+  }
+}
+GM_DEVI void store_fp_u64(uint64_t *dst, const fp_t &a) {
+#pragma unroll
+  for (int i = 0; i < NL / 2; i++) dst[i] = (uint64_t)a.v[2 * i] | ((uint64_t)a.v[2 * i + 1] << 32);
+}
+
+}  // namespace gm

@@ -1,0 +1,47 @@
+// Internal interface between the C-ABI layer (capi.cu, field_kernels.cu) and
+// the MSM engine (msm.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace gm {
+
+enum {
+  GM_OK = 0,
+  GM_ERR_ARG = -1,
+  GM_ERR_STREAM = -2,
+  GM_ERR_ALLOC = -3,
+  GM_ERR_CUDA = -4,
+  GM_ERR_CHECK = -5,
+};
+
+int record_error(cudaError_t e, const char *where);
+const char *last_error();
+int select_device(uint32_t gpu_index);
+int device_sm_count(int dev, int *sms);
+void set_last_error(const char *msg);
+
+// phase profiling: when enabled, msm_launch records a CUDA event on the
+// launching stream at every phase boundary; profile_collect synchronises
+// them and returns per-phase milliseconds.
+void profile_enable(bool on);
+bool profile_enabled();
+void profile_mark(cudaStream_t s, const char *name);
+void profile_end_call();
+int profile_collect(char *names, int names_len, float *ms, int max);
+// kernel launches issued by this host thread since the last reset
+void count_launches(int k);
+int64_t launches_and_reset();
+int pool_alloc(int dev, cudaStream_t s, size_t bytes, void **ptr);
+int default_window(int group, int64_t n, int limbs);
+
+// Full MSM pipeline on `s`.  Either `bases` (packed records) or `ref_points`
+// (reference-layout affine points; converted to Montgomery when to_mont) is
+// given.  Writes the projective result (reference layout) to out_proj.  When
+// err_out is non-null it receives the device consistency flag (0 = ok).
+template <class F>
+int msm_launch(cudaStream_t s, int dev, const uint4 *bases, const uint64_t *ref_points, int to_mont,
+               const uint64_t *scalars, int limbs, int64_t n, uint64_t *out_proj, int c_override, uint32_t *err_out);
+
+}  // namespace gm

@@ -1,0 +1,502 @@
+// Pippenger bucket-method kernels for BLS12-446 G1/G2 on sm_100a.
+//
+// Pipeline for one MSM  sum_i k_i * P_i  (replaces the per-window host loop of
+// pdroalves/gpu_msm src/curve.cu:2538-2677 and the affine multi-limb path
+// src/curve.cu:2763-2820):
+//
+//  1. k_count      signed c-bit digit decomposition of every scalar; count the
+//                  non-zero digits per global bucket key  key = w*B + |d|-1
+//                  (B = 2^(c-1) buckets per window).
+//  2. k_scan_*     exclusive prefix sum of the counts -> bucket offsets.
+//  3. k_scatter    counting-sort scatter: the (point, sign) entries land
+//                  grouped by bucket key (one radix pass over all windows).
+//  4. k_accumulate every thread sums an equal-length slice of the sorted
+//                  entries with XYZZ mixed additions; buckets that fit in a
+//                  slice are written directly, the edge pieces of buckets that
+//                  straddle slices are written as partials.
+//  5. k_fixup      the slice that opened a straddling bucket adds the
+//                  partials of the following slices.
+//  6. k_reduce     per window, sum_b b*Bucket_b by segmented running sums,
+//                  applied level by level until one (R, A) pair per window
+//                  remains; the window sum is R + A.
+//  7. k_combine    result = sum_w 2^(c*w) * S_w by Horner, converted to the
+//                  reference's homogeneous projective output.
+//
+// Packed base records (written once by k_pack_*): affine x, y in Montgomery
+// form as 32-bit limbs, then an infinity word; 128 B per G1 point and 256 B
+// per G2 point so that every record is one or two whole cache lines and is
+// read with 16-byte vector loads.
+#pragma once
+#include <cstdint>
+
+#include "xyzz.cuh"
+
+namespace gm {
+
+template <class F>
+struct Rec;
+template <>
+struct Rec<Fp> {
+  static constexpr int U4 = 8;  // 128 B
+};
+template <>
+struct Rec<Fp2> {
+  static constexpr int U4 = 16;  // 256 B
+};
+
+template <class F>
+GM_DEVI uint32_t &limb_ref(typename F::T &a, int i);
+template <>
+GM_DEVI uint32_t &limb_ref<Fp>(fp_t &a, int i) {
+  return a.v[i];
+}
+template <>
+GM_DEVI uint32_t &limb_ref<Fp2>(fp2_t &a, int i) {
+  return i < NL ? a.c0.v[i] : a.c1.v[i - NL];
+}
+
+// Load x, y of a packed record with 16-byte loads through the read-only path.
+template <class F>
+GM_DEVI void load_base(typename F::T &x, typename F::T &y, const uint4 *rec) {
+  constexpr int L = F::LIMBS;  // 32-bit words per coordinate
+#pragma unroll
+  for (int q = 0; q < L / 2; q++) {
+    const uint4 v = __ldg(rec + q);
+    const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      const int idx = 4 * q + e;
+      if (idx < L)
+        limb_ref<F>(x, idx) = w[e];
+      else
+        limb_ref<F>(y, idx - L) = w[e];
+    }
+  }
+}
+
+GM_DEVI uint32_t base_is_inf(const uint4 *rec, int u4_per_rec, int limbs) {
+  const uint32_t *w = reinterpret_cast<const uint32_t *>(rec);
+  return __ldg(w + 2 * limbs);
+}
+
+// Element in the reference layout (u64 limbs, 7 per Fp) <-> registers
+template <class F>
+GM_DEVI void load_ref(typename F::T &r, const uint64_t *src) {
+#pragma unroll
+  for (int i = 0; i < F::LIMBS / 2; i++) {
+    const uint64_t w = src[i];
+    limb_ref<F>(r, 2 * i) = (uint32_t)w;
+    limb_ref<F>(r, 2 * i + 1) = (uint32_t)(w >> 32);
+  }
+}
+template <class F>
+GM_DEVI void store_ref(uint64_t *dst, typename F::T &a) {
+#pragma unroll
+  for (int i = 0; i < F::LIMBS / 2; i++)
+    dst[i] = (uint64_t)limb_ref<F>(a, 2 * i) | ((uint64_t)limb_ref<F>(a, 2 * i + 1) << 32);
+}
+
+// to-Montgomery for either field
+template <class F>
+GM_DEVI typename F::T field_to_mont(const typename F::T &a);
+template <>
+GM_DEVI fp_t field_to_mont<Fp>(const fp_t &a) {
+  return Fp::to_mont(a);
+}
+template <>
+GM_DEVI fp2_t field_to_mont<Fp2>(const fp2_t &a) {
+  return fp2_t{Fp::to_mont(a.c0), Fp::to_mont(a.c1)};
+}
+template <class F>
+GM_DEVI typename F::T field_from_mont(const typename F::T &a);
+template <>
+GM_DEVI fp_t field_from_mont<Fp>(const fp_t &a) {
+  return Fp::from_mont(a);
+}
+template <>
+GM_DEVI fp2_t field_from_mont<Fp2>(const fp2_t &a) {
+  return fp2_t{Fp::from_mont(a.c0), Fp::from_mont(a.c1)};
+}
+
+// ---------------------------------------------------------------------------
+// 0. packing: reference affine structs -> packed records
+//    ref_stride_u64: 15 (G1Point, 120 B) or 29 (G2Point, 232 B); the
+//    infinity bool sits right after the coordinates.
+// ---------------------------------------------------------------------------
+template <class F>
+__global__ void k_pack_ref(uint4 *__restrict__ out, const uint64_t *__restrict__ pts, int64_t n,
+                           int ref_stride_u64, int to_mont) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  constexpr int L = F::LIMBS;
+  const uint64_t *src = pts + i * ref_stride_u64;
+  const uint8_t inf = reinterpret_cast<const uint8_t *>(src + L)[0];
+  typename F::T x, y;
+  load_ref<F>(x, src);
+  load_ref<F>(y, src + L / 2);
+  if (inf) {
+    x = F::zero();
+    y = F::zero();
+  } else if (to_mont) {
+    x = field_to_mont<F>(x);
+    y = field_to_mont<F>(y);
+  }
+  uint32_t w[4 * Rec<F>::U4];
+#pragma unroll
+  for (int k = 0; k < 4 * Rec<F>::U4; k++) w[k] = 0;
+#pragma unroll
+  for (int k = 0; k < L; k++) {
+    w[k] = limb_ref<F>(x, k);
+    w[L + k] = limb_ref<F>(y, k);
+  }
+  w[2 * L] = inf ? 1u : 0u;
+  uint4 *dst = out + i * Rec<F>::U4;
+#pragma unroll
+  for (int q = 0; q < Rec<F>::U4; q++) dst[q] = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
+}
+
+// ---------------------------------------------------------------------------
+// 1/3. digit decomposition
+// ---------------------------------------------------------------------------
+constexpr int MAX_SCALAR_LIMBS = 8;
+
+struct DigitParams {
+  int c;       // window width in bits
+  int W;       // number of windows
+  int B;       // buckets per window = 2^(c-1)
+  int limbs;   // u64 limbs per scalar
+};
+
+GM_DEVI uint32_t window_bits(const uint64_t s[MAX_SCALAR_LIMBS], int limbs, int off, int c) {
+  const int l = off >> 6, sh = off & 63;
+  if (l >= limbs) return 0;
+  uint64_t v = s[l] >> sh;
+  if (sh + c > 64 && l + 1 < limbs) v |= s[l + 1] << (64 - sh);
+  return (uint32_t)(v & ((1ull << c) - 1));
+}
+
+// Calls fn(w, d) for every non-zero signed digit d of the scalar, where
+// scalar = sum_w d_w 2^(c w) and |d_w| <= 2^(c-1).
+template <class Fn>
+GM_DEVI void for_each_digit(const uint64_t *__restrict__ scalar, const DigitParams &dp, Fn fn) {
+  uint64_t s[MAX_SCALAR_LIMBS];
+#pragma unroll
+  for (int l = 0; l < MAX_SCALAR_LIMBS; l++) s[l] = l < dp.limbs ? scalar[l] : 0;
+  uint32_t carry = 0;
+  for (int w = 0; w < dp.W; w++) {
+    const uint32_t v = window_bits(s, dp.limbs, w * dp.c, dp.c) + carry;
+    int d;
+    if (v > (uint32_t)dp.B) {
+      d = (int)v - 2 * dp.B;
+      carry = 1;
+    } else {
+      d = (int)v;
+      carry = 0;
+    }
+    if (d != 0) fn(w, d);
+  }
+}
+
+static __global__ void k_count(const uint64_t *__restrict__ scalars, const uint4 *__restrict__ bases, int rec_u4,
+                        int field_limbs, int64_t n, DigitParams dp, uint32_t *__restrict__ counts) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (base_is_inf(bases + i * rec_u4, rec_u4, field_limbs)) return;
+  for_each_digit(scalars + i * dp.limbs, dp, [&](int w, int d) {
+    const int b = (d < 0 ? -d : d) - 1;
+    atomicAdd(&counts[w * dp.B + b], 1u);
+  });
+}
+
+// Consumes counts back down to zero; entry = (point index << 1) | negative.
+static __global__ void k_scatter(const uint64_t *__restrict__ scalars, const uint4 *__restrict__ bases, int rec_u4,
+                          int field_limbs, int64_t n, DigitParams dp, const uint32_t *__restrict__ offsets,
+                          uint32_t *__restrict__ counts, uint32_t *__restrict__ entries) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (base_is_inf(bases + i * rec_u4, rec_u4, field_limbs)) return;
+  for_each_digit(scalars + i * dp.limbs, dp, [&](int w, int d) {
+    const int key = w * dp.B + (d < 0 ? -d : d) - 1;
+    const uint32_t rank = atomicSub(&counts[key], 1u) - 1u;
+    entries[offsets[key] + rank] = ((uint32_t)i << 1) | (d < 0 ? 1u : 0u);
+  });
+}
+
+// ---------------------------------------------------------------------------
+// 2. exclusive scan (three kernels, 1024 elements per block)
+// ---------------------------------------------------------------------------
+constexpr int SCAN_THREADS = 256;
+constexpr int SCAN_PER_THREAD = 4;
+constexpr int SCAN_TILE = SCAN_THREADS * SCAN_PER_THREAD;
+
+GM_DEVI uint32_t block_exclusive_scan(uint32_t v, uint32_t &total) {
+  __shared__ uint32_t warp_sums[SCAN_THREADS / 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warp_sums[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    uint32_t s = lane < SCAN_THREADS / 32 ? warp_sums[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= o) s += y;
+    }
+    if (lane < SCAN_THREADS / 32) warp_sums[lane] = s;
+  }
+  __syncthreads();
+  const uint32_t warp_prefix = wid > 0 ? warp_sums[wid - 1] : 0;
+  total = warp_sums[SCAN_THREADS / 32 - 1];
+  __syncthreads();
+  return warp_prefix + x - v;
+}
+
+static __global__ void k_scan_blocksum(const uint32_t *__restrict__ in, int64_t K, uint32_t *__restrict__ bsum) {
+  const int64_t base = (int64_t)blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_PER_THREAD;
+  uint32_t s = 0;
+#pragma unroll
+  for (int k = 0; k < SCAN_PER_THREAD; k++)
+    if (base + k < K) s += in[base + k];
+  uint32_t total;
+  block_exclusive_scan(s, total);
+  if (threadIdx.x == 0) bsum[blockIdx.x] = total;
+}
+
+// single block: exclusive scan of nb block sums in place
+static __global__ void k_scan_top(uint32_t *__restrict__ bsum, int nb) {
+  uint32_t running = 0;
+  for (int base = 0; base < nb; base += SCAN_TILE) {
+    const int i0 = base + threadIdx.x * SCAN_PER_THREAD;
+    uint32_t v[SCAN_PER_THREAD], s = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_PER_THREAD; k++) {
+      v[k] = (i0 + k < nb) ? bsum[i0 + k] : 0;
+      s += v[k];
+    }
+    uint32_t total;
+    uint32_t ex = block_exclusive_scan(s, total) + running;
+#pragma unroll
+    for (int k = 0; k < SCAN_PER_THREAD; k++) {
+      if (i0 + k < nb) bsum[i0 + k] = ex;
+      ex += v[k];
+    }
+    running += total;
+    __syncthreads();
+  }
+}
+
+static __global__ void k_scan_final(const uint32_t *__restrict__ in, int64_t K, const uint32_t *__restrict__ bsum,
+                             uint32_t *__restrict__ out) {
+  const int64_t base = (int64_t)blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_PER_THREAD;
+  uint32_t v[SCAN_PER_THREAD], s = 0;
+#pragma unroll
+  for (int k = 0; k < SCAN_PER_THREAD; k++) {
+    v[k] = (base + k < K) ? in[base + k] : 0;
+    s += v[k];
+  }
+  uint32_t total;
+  uint32_t ex = block_exclusive_scan(s, total) + bsum[blockIdx.x];
+#pragma unroll
+  for (int k = 0; k < SCAN_PER_THREAD; k++) {
+    if (base + k < K) out[base + k] = ex;
+    if (base + k == K - 1) out[K] = ex + v[k];
+    ex += v[k];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 4. bucket accumulation over equal slices of the sorted entries
+// ---------------------------------------------------------------------------
+GM_DEVI int64_t bucket_of(const uint32_t *__restrict__ offsets, int64_t K, uint32_t pos) {
+  // largest k in [0, K) with offsets[k] <= pos
+  int64_t lo = 0, hi = K;  // offsets[K] > pos
+  while (hi - lo > 1) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (__ldg(offsets + mid) <= pos)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+template <class F>
+__global__ void __launch_bounds__(128) k_accumulate(const uint4 *__restrict__ bases, const uint32_t *__restrict__ entries,
+                                                    const uint32_t *__restrict__ offsets, int64_t K, int64_t nthreads,
+                                                    xyzz_t<F> *__restrict__ buckets,
+                                                    xyzz_t<F> *__restrict__ part_head, xyzz_t<F> *__restrict__ part_tail,
+                                                    int32_t *__restrict__ head_key, int32_t *__restrict__ tail_key) {
+  using T = typename F::T;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nthreads) return;
+  int32_t hk = -1, tk = -1;
+  // slice length from the actual number of entries (offsets[K])
+  const uint32_t M = __ldg(offsets + K);
+  const uint64_t chunk64 = ((uint64_t)M + nthreads - 1) / nthreads;
+  const uint32_t chunk = chunk64 > 0 ? (uint32_t)chunk64 : 1u;
+  const uint64_t start64 = (uint64_t)t * chunk;
+  if (start64 < M) {
+    const uint32_t start = (uint32_t)start64;
+    const uint32_t end = (uint32_t)(start64 + chunk < M ? start64 + chunk : M);
+    int64_t k = bucket_of(offsets, K, start);
+    uint32_t bend = __ldg(offsets + k + 1);
+    bool owns = __ldg(offsets + k) == start;
+    xyzz_t<F> acc;
+    xyzz_set_inf(acc);
+    uint32_t pos = start;
+    while (true) {
+      const uint32_t e = __ldg(entries + pos);
+      T x, y;
+      load_base<F>(x, y, bases + (size_t)(e >> 1) * Rec<F>::U4);
+      if (e & 1u) y = F::neg(y);
+      xyzz_madd<F>(acc, x, y);
+      pos++;
+      if (pos == bend || pos == end) {
+        if (!owns) {
+          part_head[t] = acc;
+          hk = (int32_t)k;
+        } else if (pos == bend) {
+          buckets[k] = acc;
+        } else {
+          part_tail[t] = acc;
+          tk = (int32_t)k;
+        }
+        if (pos == end) break;
+        k++;
+        while (__ldg(offsets + k + 1) <= pos) k++;
+        bend = __ldg(offsets + k + 1);
+        owns = true;
+        xyzz_set_inf(acc);
+      }
+    }
+  }
+  head_key[t] = hk;
+  tail_key[t] = tk;
+}
+
+// 5. the slice that opened a straddling bucket folds in the following slices
+template <class F>
+__global__ void __launch_bounds__(128) k_fixup(const uint32_t *__restrict__ offsets, int64_t K, int64_t nthreads,
+                                               xyzz_t<F> *__restrict__ buckets, const xyzz_t<F> *__restrict__ part_head,
+                                               const xyzz_t<F> *__restrict__ part_tail,
+                                               const int32_t *__restrict__ head_key, const int32_t *__restrict__ tail_key,
+                                               uint32_t *__restrict__ err) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nthreads) return;
+  const int32_t k = tail_key[t];
+  if (k < 0) return;
+  const uint32_t M = __ldg(offsets + K);
+  const uint64_t chunk64 = ((uint64_t)M + nthreads - 1) / nthreads;
+  const uint32_t chunk = chunk64 > 0 ? (uint32_t)chunk64 : 1u;
+  xyzz_t<F> acc = part_tail[t];
+  const uint64_t bend = __ldg(offsets + k + 1);
+  int64_t t2 = t + 1;
+  while (t2 < nthreads) {
+    if (head_key[t2] != k) {  // cannot happen for a consistent slicing
+      atomicOr(err, 1u);
+      break;
+    }
+    xyzz_t<F> h = part_head[t2];
+    xyzz_add_cold<F>(acc, h);
+    if ((uint64_t)(t2 + 1) * chunk >= bend) break;
+    t2++;
+  }
+  buckets[k] = acc;
+}
+
+// ---------------------------------------------------------------------------
+// 6. bucket reduction: per window  S = sum_{j=0}^{B-1} (j+1) * V_j.
+//
+// Level input per window: N elements A_j (and, above level 1, carried partial
+// results R_j).  A thread takes a segment [s*L, s*L+L) and computes by a
+// running sum from the top
+//     ws = sum_j (j - s*L) * A_j,   a = sum_j A_j,   r = sum_j R_j,
+// and emits  R' = r + 2^ushift * ws,  A' = a.  With U = the product of the
+// segment lengths of the levels below,  sum_j j*V_j = sum R' + U*L * sum_s s*A'_s,
+// so the next level sees the same problem on N/L elements.  When one element
+// per window is left, S = R + A.
+// ---------------------------------------------------------------------------
+template <class F>
+__global__ void __launch_bounds__(128) k_reduce_buckets(const xyzz_t<F> *__restrict__ buckets,
+                                                        const uint32_t *__restrict__ offsets, int W, int B, int L,
+                                                        xyzz_t<F> *__restrict__ R_out, xyzz_t<F> *__restrict__ A_out) {
+  const int nseg = (B + L - 1) / L;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (int64_t)W * nseg) return;
+  const int w = (int)(t / nseg), s = (int)(t % nseg);
+  const int64_t kb = (int64_t)w * B;
+  xyzz_t<F> acc, ws;
+  xyzz_set_inf(acc);
+  xyzz_set_inf(ws);
+  const int j0 = s * L, j1 = min(B, j0 + L);
+  for (int j = j1 - 1; j >= j0; j--) {
+    if (__ldg(offsets + kb + j + 1) != __ldg(offsets + kb + j)) {
+      xyzz_t<F> v = buckets[kb + j];
+      xyzz_add_cold<F>(acc, v);
+    }
+    if (j > j0) xyzz_add_cold<F>(ws, acc);
+  }
+  R_out[t] = ws;
+  A_out[t] = acc;
+}
+
+template <class F>
+__global__ void __launch_bounds__(128) k_reduce_level(const xyzz_t<F> *__restrict__ R_in, const xyzz_t<F> *__restrict__ A_in,
+                                                      int W, int N, int L, int ushift, xyzz_t<F> *__restrict__ R_out,
+                                                      xyzz_t<F> *__restrict__ A_out) {
+  const int nseg = (N + L - 1) / L;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (int64_t)W * nseg) return;
+  const int w = (int)(t / nseg), s = (int)(t % nseg);
+  const int64_t kb = (int64_t)w * N;
+  xyzz_t<F> acc, ws, r;
+  xyzz_set_inf(acc);
+  xyzz_set_inf(ws);
+  xyzz_set_inf(r);
+  const int j0 = s * L, j1 = min(N, j0 + L);
+  for (int j = j1 - 1; j >= j0; j--) {
+    xyzz_t<F> a = A_in[kb + j];
+    xyzz_add_cold<F>(acc, a);
+    if (j > j0) xyzz_add_cold<F>(ws, acc);
+    xyzz_t<F> rr = R_in[kb + j];
+    xyzz_add_cold<F>(r, rr);
+  }
+  for (int k = 0; k < ushift; k++) xyzz_dbl_cold<F>(ws);
+  xyzz_add_cold<F>(r, ws);
+  R_out[t] = r;
+  A_out[t] = acc;
+}
+
+// 7. Horner over windows; writes the homogeneous projective result in the
+// reference layout (X, Y, Z; u64 limbs; Montgomery form).
+template <class F>
+__global__ void k_combine(const xyzz_t<F> *__restrict__ R, const xyzz_t<F> *__restrict__ A, int W, int c,
+                          uint64_t *__restrict__ out_proj, xyzz_t<F> *__restrict__ out_xyzz) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  xyzz_t<F> res;
+  xyzz_set_inf(res);
+  for (int w = W - 1; w >= 0; w--) {
+    if (!xyzz_is_inf(res))
+      for (int k = 0; k < c; k++) xyzz_dbl_cold<F>(res);
+    xyzz_t<F> s = R[w];
+    xyzz_t<F> a = A[w];
+    xyzz_add_cold<F>(s, a);
+    xyzz_add_cold<F>(res, s);
+  }
+  if (out_xyzz) *out_xyzz = res;
+  if (out_proj) {
+    typename F::T X, Y, Z;
+    xyzz_to_proj<F>(X, Y, Z, res);
+    constexpr int H = F::LIMBS / 2;  // u64 words per coordinate
+    store_ref<F>(out_proj, X);
+    store_ref<F>(out_proj + H, Y);
+    store_ref<F>(out_proj + 2 * H, Z);
+  }
+}
+
+}  // namespace gm

@@ -1,0 +1,186 @@
+/*
+ * gpu_msm_b200 -- B200-native (sm_100a) BLS12-446 multi-scalar multiplication.
+ *
+ * C-ABI of the shared library libgpu_msm_b200.so.  Plain pointers and sizes,
+ * no C++ or torch types in the signatures.
+ *
+ * Part 1 reproduces, name for name and signature for signature, the C-ABI that
+ * pdroalves/gpu_msm exports to its Rust crate (rust-api/include/rust_wrapper.h,
+ * bound by rust-api/src/ffi.rs:65-106), so an existing binding links against
+ * this library unchanged.  Part 2 adds entry points the reference does not
+ * have (full-width scalars, device-resident inputs, resident base tables,
+ * batches).  Each declaration names the reference interface it replaces.
+ *
+ * Conventions (same as the reference unless stated):
+ *   - Fp is 7 little-endian u64 limbs; points hold Montgomery-form
+ *     coordinates (R = 2^448) unless a function says "standard form".
+ *   - Affine points carry an `infinity` flag; projective points use Z = 0 for
+ *     infinity.  Struct pad bytes are never read.
+ *   - Scalars are little-endian u64 limbs, `scalar_limbs` per scalar, stored
+ *     scalar-major (scalar i occupies limbs [i*scalar_limbs, (i+1)*scalar_limbs)).
+ *   - MSM results are homogeneous projective points; (X, Y, Z) is a valid
+ *     representation of the sum, not a specific one, so results are compared
+ *     after conversion to affine.
+ *   - Status codes of the int-returning functions: 0 ok, -1 bad size/argument,
+ *     -2 stream creation failed, -3 allocation failed, -4 CUDA error,
+ *     -5 device consistency check failed.
+ */
+#ifndef GPU_MSM_B200_H
+#define GPU_MSM_B200_H
+
+#include <stdbool.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Types: byte-compatible with include/fp.h:13, include/fp2.h:10 and
+ * include/curve.h:13-43 of the reference (sizes 56/112/120/232/168/336 B). */
+typedef struct Fp { uint64_t limb[7]; } Fp;
+typedef struct Fp2 { Fp c0; Fp c1; } Fp2;
+typedef struct G1Point { Fp x; Fp y; bool infinity; } G1Point;
+typedef struct G2Point { Fp2 x; Fp2 y; bool infinity; } G2Point;
+typedef struct G1ProjectivePoint { Fp X; Fp Y; Fp Z; } G1ProjectivePoint;
+typedef struct G2ProjectivePoint { Fp2 X; Fp2 Y; Fp2 Z; } G2ProjectivePoint;
+
+typedef struct CUstream_st *gm_stream_t; /* a cudaStream_t */
+
+/* ======================================================================== */
+/* Part 1: the reference C-ABI (rust-api/include/rust_wrapper.h)             */
+/* ======================================================================== */
+
+/* rust_wrapper.h:14 -- Z = 1 (Montgomery); infinity -> (0, 0, 0) */
+void affine_to_projective_g1_wrapper(G1ProjectivePoint *proj, const G1Point *affine);
+/* rust_wrapper.h:17 */
+void affine_to_projective_g2_wrapper(G2ProjectivePoint *proj, const G2Point *affine);
+/* rust_wrapper.h:20 -- x = X/Z, y = Y/Z (Montgomery); Z = 0 -> infinity */
+void projective_to_affine_g1_wrapper(G1Point *affine, const G1ProjectivePoint *proj);
+/* rust_wrapper.h:23 */
+void projective_to_affine_g2_wrapper(G2Point *affine, const G2ProjectivePoint *proj);
+/* rust_wrapper.h:26-35 */
+void g1_point_at_infinity_wrapper(G1Point *point);
+void g2_point_at_infinity_wrapper(G2Point *point);
+void g1_projective_point_at_infinity_wrapper(G1ProjectivePoint *point);
+void g2_projective_point_at_infinity_wrapper(G2ProjectivePoint *point);
+/* rust_wrapper.h:38-41 */
+bool g1_is_infinity_wrapper(const G1Point *point);
+bool g2_is_infinity_wrapper(const G2Point *point);
+
+/* rust_wrapper.h:45 (c_wrapper.cu:64-172): host buffers, u64 scalars.
+ * Points arrive in STANDARD form and are converted to Montgomery on the
+ * device (c_wrapper.cu:127).  Returns 0, or -1 when n <= 0. */
+int g1_msm_wrapper(G1ProjectivePoint *result, const G1Point *points, const uint64_t *scalars, int n,
+                   uint32_t gpu_index);
+/* rust_wrapper.h:53 (c_wrapper.cu:175-258): host buffers, u64 scalars.
+ * Points are taken as already in Montgomery form (no conversion,
+ * c_wrapper.cu:223-224), as in the reference. */
+int g2_msm_wrapper(G2ProjectivePoint *result, const G2Point *points, const uint64_t *scalars, int n,
+                   uint32_t gpu_index);
+
+/* rust_wrapper.h:63-65 (c_wrapper.cu:261-288) */
+void g1_from_montgomery_wrapper(G1Point *result, const G1Point *point);
+void g2_from_montgomery_wrapper(G2Point *result, const G2Point *point);
+void fp_to_montgomery_wrapper(Fp *result, const Fp *value);
+
+/* include/curve.h:108 (src/curve.cu:833); bound with C linkage by
+ * rust-api/src/ffi.rs:67.  Kept for link compatibility: the generators are
+ * compile-time constants here, so this only validates the device index. */
+void init_device_generators(gm_stream_t stream, uint32_t gpu_index);
+
+/* ======================================================================== */
+/* Part 2: additive entry points                                             */
+/* ======================================================================== */
+
+/* Full-width host-buffer MSM.  Replaces point_msm<G1Point>/<G2Point>
+ * (include/curve.h:238-241, src/curve.cu:2763-2826) for callers of the
+ * C-ABI, which the reference restricts to u64 scalars.  points_montgomery != 0:
+ * points are in Montgomery form; 0: standard form (converted on device).
+ * 1 <= scalar_limbs <= 8.  n == 0 yields infinity. */
+int g1_msm_limbs_wrapper(G1ProjectivePoint *result, const G1Point *points, const uint64_t *scalars,
+                         int scalar_limbs, int n, uint32_t gpu_index, int points_montgomery);
+int g2_msm_limbs_wrapper(G2ProjectivePoint *result, const G2Point *points, const uint64_t *scalars,
+                         int scalar_limbs, int n, uint32_t gpu_index, int points_montgomery);
+
+/* Device-pointer MSM, asynchronous on `stream`.  Replaces
+ * point_msm_u64_async_g1/_g2 (include/curve.h:232-235; scalar_limbs = 1) and
+ * point_msm_async<G1Point>/<G2Point> (include/curve.h:238) without the
+ * caller-sized scratch buffer: workspace comes from a per-device stream-
+ * ordered pool.  d_points: reference-layout affine points, Montgomery form. */
+int gm_g1_msm_device(gm_stream_t stream, uint32_t gpu_index, G1ProjectivePoint *d_result, const G1Point *d_points,
+                     const uint64_t *d_scalars, int scalar_limbs, int n);
+int gm_g2_msm_device(gm_stream_t stream, uint32_t gpu_index, G2ProjectivePoint *d_result, const G2Point *d_points,
+                     const uint64_t *d_scalars, int scalar_limbs, int n);
+
+/* Same, with explicit window width c (2..20); 0 picks c from the cost
+ * model.  Used by the autotuner and by parity tests that sweep c. */
+int gm_g1_msm_device_c(gm_stream_t stream, uint32_t gpu_index, G1ProjectivePoint *d_result, const G1Point *d_points,
+                       const uint64_t *d_scalars, int scalar_limbs, int n, int window_bits);
+int gm_g2_msm_device_c(gm_stream_t stream, uint32_t gpu_index, G2ProjectivePoint *d_result, const G2Point *d_points,
+                       const uint64_t *d_scalars, int scalar_limbs, int n, int window_bits);
+
+/* Window width the cost model picks for an MSM of n points (group 1 or 2). */
+int gm_msm_default_window(int group, int64_t n, int scalar_limbs);
+
+/* Fp microbench kernels (device pointers, asynchronous).
+ * gm_fp_mont_mul_array: c[i] = a[i]*b[i]*R^-1 (Montgomery form), the
+ *   batched form of fp_mont_mul (src/fp.cu:370).
+ * gm_fp_mul_array: c[i] = a[i]*b[i] mod p on standard-form values, the
+ *   C-ABI form of fp_mul_array_device (include/fp_kernels.h:39).
+ * gm_fp2_mont_mul_array: batched fp2_mont_mul (src/fp2.cu:88).
+ * gm_fp2_mul_array: batched normal-form fp2_mul on device pointers, the
+ *   device-resident form of fp2_mul_array_host (include/fp2_kernels.h:19). */
+int gm_fp_mont_mul_array(gm_stream_t stream, uint32_t gpu_index, Fp *d_c, const Fp *d_a, const Fp *d_b, int64_t n);
+int gm_fp_mul_array(gm_stream_t stream, uint32_t gpu_index, Fp *d_c, const Fp *d_a, const Fp *d_b, int64_t n);
+int gm_fp2_mont_mul_array(gm_stream_t stream, uint32_t gpu_index, Fp2 *d_c, const Fp2 *d_a, const Fp2 *d_b, int64_t n);
+int gm_fp2_mul_array(gm_stream_t stream, uint32_t gpu_index, Fp2 *d_c, const Fp2 *d_a, const Fp2 *d_b, int64_t n);
+
+/* Batched standard <-> Montgomery conversion of reference-layout affine
+ * points in place (device pointers).  Replaces point_to_montgomery_batch
+ * (include/curve.h:207, src/curve.cu:2506); from_montgomery has no batched
+ * counterpart in the reference (src/curve.cu:2356 is never launched). */
+int gm_g1_to_montgomery_batch(gm_stream_t stream, uint32_t gpu_index, G1Point *d_points, int n);
+int gm_g2_to_montgomery_batch(gm_stream_t stream, uint32_t gpu_index, G2Point *d_points, int n);
+
+/* Fixed-base batch: out[i] = k_i * G (Montgomery affine, canonical), for the
+ * generator G of src/curve.cu:786-814.  No reference counterpart beyond the
+ * single-point point_scalar_mul (src/curve.cu:230); used to build synthetic
+ * base tables P_i = k_i * G on the device. */
+int gm_g1_generator_mul_batch(gm_stream_t stream, uint32_t gpu_index, G1Point *d_out, const uint64_t *d_scalars,
+                              int scalar_limbs, int n);
+int gm_g2_generator_mul_batch(gm_stream_t stream, uint32_t gpu_index, G2Point *d_out, const uint64_t *d_scalars,
+                              int scalar_limbs, int n);
+
+/* d_out = sum of n projective points (device pointers, one thread).  Adds
+ * the partial MSM results of shards computed on several devices or in
+ * several batches; the reference has no sharded MSM. */
+int gm_g1_sum_projective(gm_stream_t stream, uint32_t gpu_index, G1ProjectivePoint *d_out,
+                         const G1ProjectivePoint *d_in, int n);
+int gm_g2_sum_projective(gm_stream_t stream, uint32_t gpu_index, G2ProjectivePoint *d_out,
+                         const G2ProjectivePoint *d_in, int n);
+
+/* Measurement hooks (no reference counterpart).
+ * gm_profile_enable: while on, every MSM records CUDA events on its stream at
+ *   its phase boundaries (pack, sort, accumulate, fixup, reduce, combine).
+ * gm_profile_collect: waits for those events and returns up to `max`
+ *   per-phase milliseconds in launch order, with their names comma-separated
+ *   in `names`; clears the record.
+ * gm_launch_count_reset: number of kernels this library launched from the
+ *   calling thread since the previous call.
+ * gm_imad_probe: launches a kernel of independent 32-bit IMAD chains over
+ *   the whole GPU; *imad_per_launch receives the IMAD count so that the caller
+ *   can time it and derive the integer multiply-add peak. */
+int gm_profile_enable(int on);
+int gm_profile_collect(char *names, int names_len, float *ms, int max);
+int64_t gm_launch_count_reset(void);
+int gm_imad_probe(gm_stream_t stream, uint32_t gpu_index, int iters, uint32_t *d_sink, int64_t sink_words,
+                  int64_t *imad_per_launch);
+
+/* Last CUDA error string seen by this library on the calling thread. */
+const char *gm_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GPU_MSM_B200_H */

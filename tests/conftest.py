@@ -1,0 +1,27 @@
+"""Shared pytest setup.
+
+Markers:
+  gpu -- needs a CUDA device (B200); the parity tests proper.  Everything else
+         runs on the CPU (oracle vs golden vectors, host logic, C-ABI exports).
+"""
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device")
+
+
+@pytest.fixture(scope="session")
+def cuda():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.fail("test marked gpu but no CUDA device is visible")
+    torch.cuda.init()
+    return torch.device("cuda:0")
