@@ -233,6 +233,18 @@ def canonical_affine(proj: np.ndarray, group: int = 1) -> np.ndarray:
 # device-resident API (torch tensors as buffers, current torch stream)
 # ---------------------------------------------------------------------------
 
+def _require(t, cols, what, rows=None):
+    """Shape/dtype/device checks before a device pointer crosses the ABI:
+    a mismatched buffer would otherwise be read out of bounds on the GPU."""
+    import torch
+    if not isinstance(t, torch.Tensor) or t.dtype != torch.int64 or not t.is_cuda or not t.is_contiguous():
+        raise ValueError(f"{what}: expected a contiguous int64 CUDA tensor")
+    if t.dim() != 2 or (cols is not None and t.shape[1] != cols):
+        raise ValueError(f"{what}: expected shape (n, {cols}), got {tuple(t.shape)}")
+    if rows is not None and t.shape[0] != rows:
+        raise ValueError(f"{what}: expected {rows} rows, got {t.shape[0]}")
+
+
 def _stream_handle(stream=None):
     import torch
     s = stream if stream is not None else torch.cuda.current_stream()
@@ -251,11 +263,19 @@ def msm_device(points, scalars, group: int = 1, window_bits: int = 0, out=None, 
     returns: int64 tensor (21,) or (42,) -- projective result, Montgomery form
     """
     import torch
+    _require(points, G1_WORDS if group == 1 else G2_WORDS, "points")
     n = points.shape[0]
-    limbs = scalars.shape[1] if scalars.dim() == 2 else 1
+    _require(scalars, None, "scalars", rows=n)
+    limbs = scalars.shape[1]
+    if not 1 <= limbs <= 8:
+        raise ValueError("scalars: 1..8 limbs per scalar")
+    if scalars.device != points.device:
+        raise ValueError("points and scalars must be on the same device")
     words = G1P_WORDS if group == 1 else G2P_WORDS
     if out is None:
         out = torch.empty(words, dtype=torch.int64, device=points.device)
+    if out.numel() < words or out.dtype != torch.int64 or out.device != points.device:
+        raise ValueError("out: int64 tensor of the result size on the points' device")
     fn = lib().gm_g1_msm_device_c if group == 1 else lib().gm_g2_msm_device_c
     _check(fn(_stream_handle(stream), _dev_index(points), ctypes.c_void_p(out.data_ptr()),
               ctypes.c_void_p(points.data_ptr()), ctypes.c_void_p(scalars.data_ptr()), limbs, n, window_bits),
@@ -267,8 +287,11 @@ def sum_projective(points, group: int = 1, out=None, stream=None):
     """Device sum of projective points (int64 tensor (k, 21) or (k, 42))."""
     import torch
     words = G1P_WORDS if group == 1 else G2P_WORDS
+    _require(points, words, "points")
     if out is None:
         out = torch.empty(words, dtype=torch.int64, device=points.device)
+    if out.numel() < words or out.dtype != torch.int64:
+        raise ValueError("out: int64 tensor of the result size")
     fn = lib().gm_g1_sum_projective if group == 1 else lib().gm_g2_sum_projective
     _check(fn(_stream_handle(stream), _dev_index(points), ctypes.c_void_p(out.data_ptr()),
               ctypes.c_void_p(points.data_ptr()), points.shape[0]), "sum_projective")
@@ -278,8 +301,11 @@ def sum_projective(points, group: int = 1, out=None, stream=None):
 def generator_mul_batch(scalars, group: int = 1, stream=None):
     """out[i] = scalars[i] * G (canonical Montgomery affine) on the device."""
     import torch
+    _require(scalars, None, "scalars")
     n = scalars.shape[0]
     limbs = scalars.shape[1]
+    if not 1 <= limbs <= 8:
+        raise ValueError("scalars: 1..8 limbs per scalar")
     words = G1_WORDS if group == 1 else G2_WORDS
     out = torch.empty((n, words), dtype=torch.int64, device=scalars.device)
     fn = lib().gm_g1_generator_mul_batch if group == 1 else lib().gm_g2_generator_mul_batch
@@ -289,6 +315,7 @@ def generator_mul_batch(scalars, group: int = 1, stream=None):
 
 
 def to_montgomery_batch(points, group: int = 1, stream=None):
+    _require(points, G1_WORDS if group == 1 else G2_WORDS, "points")
     fn = lib().gm_g1_to_montgomery_batch if group == 1 else lib().gm_g2_to_montgomery_batch
     _check(fn(_stream_handle(stream), _dev_index(points), ctypes.c_void_p(points.data_ptr()), points.shape[0]),
            "to_montgomery_batch")
@@ -299,8 +326,12 @@ def field_mul_array(a, b, op: str = "fp_mont_mul", out=None, stream=None):
     """Element-wise field products on device tensors of shape (n, 7) [Fp] or
     (n, 14) [Fp2], int64.  op: fp_mont_mul | fp_mul | fp2_mont_mul | fp2_mul."""
     import torch
+    cols = 7 if op.startswith("fp_") else 14
+    _require(a, cols, "a")
+    _require(b, cols, "b", rows=a.shape[0])
     if out is None:
         out = torch.empty_like(a)
+    _require(out, cols, "out", rows=a.shape[0])
     fn = getattr(lib(), f"gm_{op}_array")
     _check(fn(_stream_handle(stream), _dev_index(a), ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(a.data_ptr()),
               ctypes.c_void_p(b.data_ptr()), a.shape[0]), op)
@@ -344,6 +375,9 @@ def launch_count_reset() -> int:
 
 def imad_probe(iters: int, sink, stream=None) -> int:
     """Launch the IMAD throughput probe; returns IMADs per launch."""
+    import torch
+    if not (isinstance(sink, torch.Tensor) and sink.is_cuda and sink.dtype == torch.int32):
+        raise ValueError("sink: int32 CUDA tensor")
     cnt = ctypes.c_int64(0)
     _check(lib().gm_imad_probe(_stream_handle(stream), _dev_index(sink), iters, ctypes.c_void_p(sink.data_ptr()),
                                sink.numel(), ctypes.byref(cnt)), "imad_probe")

@@ -377,6 +377,20 @@ struct Fp {
   }
 };
 
+// Same field with the multiplication out of line: one copy of the ~900
+// instruction Montgomery product per kernel instead of one per call site.
+// Operands and result travel in registers (no stack frame), and the loop body
+// of the bucket accumulation then fits the instruction cache.
+static __device__ __noinline__ fp_t fp_mul_call(fp_t a, fp_t b) {
+  fp_t r;
+  mont_mul_raw<true>(r.v, a.v, b.v);
+  return r;
+}
+struct FpOut : Fp {
+  GM_DEVI static fp_t mul(const fp_t &a, const fp_t &b) { return fp_mul_call(a, b); }
+  GM_DEVI static fp_t sqr(const fp_t &a) { return fp_mul_call(a, a); }
+};
+
 // 16-byte vector loads/stores of field elements (56 B = 3.5 x 16 B, so
 // records are laid out with 16-byte alignment by the packers).
 GM_DEVI void load_fp_u64(fp_t &r, const uint64_t *src) {

@@ -64,19 +64,20 @@ int launch_field(gm_stream_t stream, uint32_t gpu_index, void *c, const void *a,
   return e == cudaSuccess ? gm::GM_OK : gm::record_error(e, "k_field_mul");
 }
 
-// IMAD-pipe throughput probe: 16 independent accumulators per thread, each
-// iteration issuing 8 mad.lo.u32 and 8 mad.hi.u32 (16 IMAD).  Used to measure
-// the integer multiply-add peak that the MSM roofline is quoted against.
+// IMAD-pipe throughput probe: 16 independent accumulator chains per thread,
+// each iteration issuing 8 mad.lo.u32 and 8 mad.hi.u32 (16 IMAD) whose only
+// dependency is on the same chain's previous value.  Used to measure the
+// integer multiply-add peak that the MSM roofline is quoted against.
 __global__ void __launch_bounds__(256) k_imad_probe(uint32_t *__restrict__ sink, int iters, uint32_t seed) {
   uint32_t a[16];
 #pragma unroll
   for (int k = 0; k < 16; k++) a[k] = seed * (threadIdx.x + 1) + 0x9e3779b9u * (k + 1);
-  const uint32_t m = seed | 1u;
+  const uint32_t m = seed | 1u, c = seed ^ 0x85ebca6bu;
   for (int it = 0; it < iters; it++) {
 #pragma unroll
     for (int k = 0; k < 16; k += 2) {
-      asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(a[k]) : "r"(m), "r"(a[k + 1]));
-      asm volatile("mad.hi.u32 %0, %0, %1, %2;" : "+r"(a[k + 1]) : "r"(m), "r"(a[k]));
+      asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(a[k]) : "r"(m), "r"(c));
+      asm volatile("mad.hi.u32 %0, %0, %1, %2;" : "+r"(a[k + 1]) : "r"(m), "r"(c));
     }
   }
   uint32_t x = 0;

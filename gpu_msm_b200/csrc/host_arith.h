@@ -171,3 +171,163 @@ inline void fp2_inv(Fp2 &c, const Fp2 &a) {
 }
 
 }  // namespace gm_host
+
+// ---------------------------------------------------------------------------
+// Host XYZZ arithmetic for the window combination of a single MSM (the
+// serial tail: ~300 doublings).  A CPU core multiplies 446-bit numbers with
+// far lower latency than one GPU thread, so the tail runs here, stream-
+// ordered through cudaLaunchHostFunc.  Same EFD formulas as xyzz.cuh:
+// dbl-2008-s-1 and add-2008-s for a = 0, all values canonical (< p).
+// ---------------------------------------------------------------------------
+namespace gm_host {
+
+struct HFp {
+  uint64_t v[L];
+};
+struct HFp2 {
+  HFp c0, c1;
+};
+
+struct F1 {
+  using T = HFp;
+  static constexpr int WORDS = L;
+  static void zero(T &a) { memset(a.v, 0, sizeof(a.v)); }
+  static bool is_zero(const T &a) { return gm_host::is_zero(a.v); }
+  static void add(T &c, const T &a, const T &b) { gm_host::add(c.v, a.v, b.v); }
+  static void sub(T &c, const T &a, const T &b) { gm_host::sub(c.v, a.v, b.v); }
+  static void mul(T &c, const T &a, const T &b) { gm_host::mont_mul(c.v, a.v, b.v); }
+};
+
+struct F2 {
+  using T = HFp2;
+  static constexpr int WORDS = 2 * L;
+  static void zero(T &a) { memset(&a, 0, sizeof(a)); }
+  static bool is_zero(const T &a) { return gm_host::is_zero(a.c0.v) && gm_host::is_zero(a.c1.v); }
+  static void add(T &c, const T &a, const T &b) {
+    gm_host::add(c.c0.v, a.c0.v, b.c0.v);
+    gm_host::add(c.c1.v, a.c1.v, b.c1.v);
+  }
+  static void sub(T &c, const T &a, const T &b) {
+    gm_host::sub(c.c0.v, a.c0.v, b.c0.v);
+    gm_host::sub(c.c1.v, a.c1.v, b.c1.v);
+  }
+  static void mul(T &c, const T &a, const T &b) {
+    uint64_t t0[L], t1[L], s0[L], s1[L], t2[L];
+    mont_mul(t0, a.c0.v, b.c0.v);
+    mont_mul(t1, a.c1.v, b.c1.v);
+    gm_host::add(s0, a.c0.v, a.c1.v);
+    gm_host::add(s1, b.c0.v, b.c1.v);
+    mont_mul(t2, s0, s1);
+    gm_host::sub(c.c0.v, t0, t1);
+    gm_host::sub(c.c1.v, t2, t0);
+    gm_host::sub(c.c1.v, c.c1.v, t1);
+  }
+};
+
+template <class F>
+struct HXyzz {
+  typename F::T X, Y, ZZ, ZZZ;
+};
+
+template <class F>
+inline bool hx_is_inf(const HXyzz<F> &p) {
+  return F::is_zero(p.ZZ);
+}
+
+template <class F>
+inline void hx_dbl(HXyzz<F> &p) {
+  using T = typename F::T;
+  if (hx_is_inf(p)) return;
+  T U, V, W, S, xx, M, t, X3, Y3;
+  F::add(U, p.Y, p.Y);
+  F::mul(V, U, U);
+  F::mul(W, U, V);
+  F::mul(S, p.X, V);
+  F::mul(xx, p.X, p.X);
+  F::add(M, xx, xx);
+  F::add(M, M, xx);
+  F::mul(X3, M, M);
+  F::add(t, S, S);
+  F::sub(X3, X3, t);
+  F::sub(t, S, X3);
+  F::mul(Y3, M, t);
+  F::mul(t, W, p.Y);
+  F::sub(Y3, Y3, t);
+  F::mul(p.ZZ, V, p.ZZ);
+  F::mul(p.ZZZ, W, p.ZZZ);
+  p.X = X3;
+  p.Y = Y3;
+}
+
+template <class F>
+inline void hx_add(HXyzz<F> &acc, const HXyzz<F> &q) {
+  using T = typename F::T;
+  if (hx_is_inf(q)) return;
+  if (hx_is_inf(acc)) {
+    acc = q;
+    return;
+  }
+  T U1, U2, S1, S2, P, R, PP, PPP, Q, X3, Y3, t;
+  F::mul(U1, acc.X, q.ZZ);
+  F::mul(U2, q.X, acc.ZZ);
+  F::mul(S1, acc.Y, q.ZZZ);
+  F::mul(S2, q.Y, acc.ZZZ);
+  F::sub(P, U2, U1);
+  F::sub(R, S2, S1);
+  if (F::is_zero(P)) {
+    if (F::is_zero(R)) {
+      hx_dbl(acc);
+    } else {
+      F::zero(acc.X);
+      F::zero(acc.Y);
+      F::zero(acc.ZZ);
+      F::zero(acc.ZZZ);
+    }
+    return;
+  }
+  F::mul(PP, P, P);
+  F::mul(PPP, P, PP);
+  F::mul(Q, U1, PP);
+  F::mul(X3, R, R);
+  F::sub(X3, X3, PPP);
+  F::add(t, Q, Q);
+  F::sub(X3, X3, t);
+  F::sub(t, Q, X3);
+  F::mul(Y3, R, t);
+  F::mul(t, S1, PPP);
+  F::sub(Y3, Y3, t);
+  F::mul(t, acc.ZZ, q.ZZ);
+  F::mul(acc.ZZ, t, PP);
+  F::mul(t, acc.ZZZ, q.ZZZ);
+  F::mul(acc.ZZZ, t, PPP);
+  acc.X = X3;
+  acc.Y = Y3;
+}
+
+// result = sum_w 2^(c w) S_w (Horner, MSB first), then to homogeneous
+// projective (X*ZZZ, Y*ZZ, ZZ*ZZZ); infinity -> all zero.  `sums` holds W
+// device-layout XYZZ points (32-bit limb order == 64-bit limb order on a
+// little-endian host); `out` receives 3 coordinates of F::WORDS u64.
+template <class F>
+inline void horner_to_proj(uint64_t *out, const HXyzz<F> *sums, int W, int c) {
+  HXyzz<F> res;
+  memset(&res, 0, sizeof(res));
+  for (int w = W - 1; w >= 0; w--) {
+    if (!hx_is_inf(res))
+      for (int k = 0; k < c; k++) hx_dbl(res);
+    hx_add(res, sums[w]);
+  }
+  typename F::T X, Y, Z;
+  if (hx_is_inf(res)) {
+    memset(out, 0, 3 * F::WORDS * sizeof(uint64_t));
+    return;
+  }
+  F::mul(X, res.X, res.ZZZ);
+  F::mul(Y, res.Y, res.ZZ);
+  F::mul(Z, res.ZZ, res.ZZZ);
+  memcpy(out, &X, F::WORDS * 8);
+  memcpy(out + F::WORDS, &Y, F::WORDS * 8);
+  memcpy(out + 2 * F::WORDS, &Z, F::WORDS * 8);
+}
+
+}  // namespace gm_host

@@ -146,6 +146,89 @@ int64_t launches_and_reset() {
   return v;
 }
 
+// ---------------------------------------------------------------------------
+// host tail: pinned slots and stream-ordered host functions
+// ---------------------------------------------------------------------------
+static constexpr size_t TAIL_SLOT_BYTES = 128 * 1024;  // >= 257 windows x 448 B + 336 B
+static std::mutex g_pin_mu;
+static std::vector<void *> g_pin_free;
+static bool g_host_tail = true;
+
+bool host_tail_enabled() { return g_host_tail; }
+void set_host_tail_enabled(bool on) { g_host_tail = on; }
+
+static int pinned_acquire(void **p) {
+  {
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    if (!g_pin_free.empty()) {
+      *p = g_pin_free.back();
+      g_pin_free.pop_back();
+      return GM_OK;
+    }
+  }
+  cudaError_t e = cudaMallocHost(p, TAIL_SLOT_BYTES);
+  if (e != cudaSuccess) return record_error(e, "cudaMallocHost(tail slot)");
+  return GM_OK;
+}
+
+static void pinned_release(void *p) {
+  std::lock_guard<std::mutex> lk(g_pin_mu);
+  g_pin_free.push_back(p);
+}
+
+struct TailCtx {
+  int group, W, c;
+  char *slot;
+};
+
+static void CUDART_CB tail_compute(void *p) {
+  auto *t = static_cast<TailCtx *>(p);
+  if (t->group == 1) {
+    uint64_t *out = reinterpret_cast<uint64_t *>(t->slot + (size_t)t->W * sizeof(gm_host::HXyzz<gm_host::F1>));
+    gm_host::horner_to_proj<gm_host::F1>(out, reinterpret_cast<const gm_host::HXyzz<gm_host::F1> *>(t->slot), t->W,
+                                         t->c);
+  } else {
+    uint64_t *out = reinterpret_cast<uint64_t *>(t->slot + (size_t)t->W * sizeof(gm_host::HXyzz<gm_host::F2>));
+    gm_host::horner_to_proj<gm_host::F2>(out, reinterpret_cast<const gm_host::HXyzz<gm_host::F2> *>(t->slot), t->W,
+                                         t->c);
+  }
+}
+
+static void CUDART_CB tail_release(void *p) {
+  auto *t = static_cast<TailCtx *>(p);
+  pinned_release(t->slot);
+  delete t;
+}
+
+int enqueue_host_tail(cudaStream_t s, int group, const void *d_sums, int W, int c, uint64_t *d_out) {
+  const size_t elem = group == 1 ? sizeof(gm_host::HXyzz<gm_host::F1>) : sizeof(gm_host::HXyzz<gm_host::F2>);
+  const size_t out_bytes = 3 * (group == 1 ? 7 : 14) * sizeof(uint64_t);
+  if ((size_t)W * elem + out_bytes > TAIL_SLOT_BYTES) {
+    set_last_error("too many windows for the host tail slot");
+    return GM_ERR_ARG;
+  }
+  void *slot = nullptr;
+  int rc = pinned_acquire(&slot);
+  if (rc) return rc;
+  auto *t = new TailCtx{group, W, c, static_cast<char *>(slot)};
+  cudaError_t e = cudaMemcpyAsync(slot, d_sums, (size_t)W * elem, cudaMemcpyDeviceToHost, s);
+  if (e != cudaSuccess) {
+    pinned_release(slot);
+    delete t;
+    return record_error(e, "tail D2H");
+  }
+  e = cudaLaunchHostFunc(s, tail_compute, t);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(d_out, static_cast<char *>(slot) + (size_t)W * elem, out_bytes, cudaMemcpyHostToDevice, s);
+  cudaError_t e2 = cudaLaunchHostFunc(s, tail_release, t);
+  if (e2 != cudaSuccess) {
+    // the slot stays with the stream's pending work; leak it rather than
+    // hand it out again while a copy may still read it
+    return record_error(e2, "tail release");
+  }
+  return e == cudaSuccess ? GM_OK : record_error(e, "tail host function");
+}
+
 int device_sm_count(int dev, int *sms) {
   DeviceState *st;
   int rc = device_state(dev, &st);

@@ -30,6 +30,13 @@ bool profile_enabled();
 void profile_mark(cudaStream_t s, const char *name);
 void profile_end_call();
 int profile_collect(char *names, int names_len, float *ms, int max);
+// Serial window combination of one MSM on the host: copies the W window
+// sums (device XYZZ) to a pinned slot, runs Horner in a stream-ordered host
+// function and copies the projective result to d_out.  Not used while the
+// stream is being captured.
+int enqueue_host_tail(cudaStream_t s, int group, const void *d_sums, int W, int c, uint64_t *d_out);
+bool host_tail_enabled();
+void set_host_tail_enabled(bool on);
 // kernel launches issued by this host thread since the last reset
 void count_launches(int k);
 int64_t launches_and_reset();

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <mutex>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -45,9 +46,10 @@ template <class F>
 struct MsmLayout {
   DigitParams dp;
   int64_t K = 0, nthreads = 0, n = 0;
-  int L1 = 8, Lk = 4;
-  std::vector<int> level_N;  // element count per window entering each level
-  size_t o_counts, o_offsets, o_bsum, o_entries, o_buckets, o_head, o_tail, o_hk, o_tk, o_red[4], o_err, o_packed;
+  int L1 = 8;     // buckets per reduction segment
+  int FAN = 4;    // fan-in of the segment-share tree
+  int nseg = 0;   // reduction segments per window
+  size_t o_counts, o_offsets, o_bsum, o_entries, o_buckets, o_head, o_tail, o_hk, o_tk, o_red[3], o_err, o_packed;
   size_t bytes = 0;
   int64_t nb = 0;
   int64_t red_elems = 0;
@@ -62,21 +64,13 @@ struct MsmLayout {
     dp.limbs = limbs;
     K = (int64_t)dp.W * dp.B;
     nb = (K + SCAN_TILE - 1) / SCAN_TILE;
-    nthreads = (int64_t)sms * std::max(1, acc_blocks_per_sm) * 128;
+    nthreads = (int64_t)sms * std::max(1, acc_blocks_per_sm) * ACC_THREADS;
     // never more slices than entries
     const int64_t max_entries = n * dp.W;
     if (nthreads > max_entries) nthreads = std::max<int64_t>(1, (max_entries + 127) / 128 * 128);
-    level_N.clear();
-    int64_t N = dp.B;
-    int L = std::min<int64_t>(L1, N);
-    red_elems = dp.W * ((N + L - 1) / L);
-    N = (N + L - 1) / L;
-    level_N.push_back((int)N);
-    while (N > 1) {
-      L = (int)std::min<int64_t>(Lk, N);
-      N = (N + L - 1) / L;
-      level_N.push_back((int)N);
-    }
+    L1 = std::min(L1, dp.B);
+    nseg = (dp.B + L1 - 1) / L1;
+    red_elems = (int64_t)dp.W * nseg;
     Carve cv;
     o_counts = cv.take<uint32_t>(K);
     o_offsets = cv.take<uint32_t>(K + 1);
@@ -87,22 +81,32 @@ struct MsmLayout {
     o_tail = cv.take<xyzz_t<F>>(nthreads);
     o_hk = cv.take<int32_t>(nthreads);
     o_tk = cv.take<int32_t>(nthreads);
-    for (int k = 0; k < 4; k++) o_red[k] = cv.take<xyzz_t<F>>(red_elems);
+    o_red[0] = cv.take<xyzz_t<F>>(red_elems);
+    o_red[1] = cv.take<xyzz_t<F>>((red_elems + FAN - 1) / FAN + dp.W);
+    o_red[2] = cv.take<xyzz_t<F>>((red_elems + FAN - 1) / FAN + dp.W);
     o_err = cv.take<uint32_t>(4);
     o_packed = pack ? cv.take<uint4>((size_t)n * Rec<F>::U4) : 0;
     bytes = cv.off;
   }
 };
 
+// Blocks of k_accumulate resident per SM; the dynamic shared-memory opt-in is
+// a per-device function attribute, so it is set (and cached) per device.
 template <class F>
-static int acc_blocks_per_sm() {
-  static int cached = -1;
-  if (cached < 0) {
+static int acc_blocks_per_sm(int dev) {
+  static std::mutex mu;
+  static int cached[64] = {0};
+  std::lock_guard<std::mutex> lk(mu);
+  if (dev < 0 || dev >= 64) dev = 0;
+  if (cached[dev] == 0) {
     int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_accumulate<F>, 128, 0) != cudaSuccess) b = 1;
-    cached = std::max(1, b);
+    cudaFuncSetAttribute(k_accumulate<F>, cudaFuncAttributeMaxDynamicSharedMemorySize, acc_smem_bytes<F>());
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_accumulate<F>, ACC_THREADS, acc_smem_bytes<F>()) !=
+        cudaSuccess)
+      b = 1;
+    cached[dev] = std::max(1, b);
   }
-  return cached;
+  return cached[dev];
 }
 
 static inline unsigned grid_for(int64_t n, int block) { return (unsigned)((n + block - 1) / block); }
@@ -131,7 +135,7 @@ int msm_launch(cudaStream_t s, int dev, const uint4 *bases, const uint64_t *ref_
     return GM_ERR_ARG;
   }
   MsmLayout<F> lay;
-  lay.plan(n, limbs, c, sms, acc_blocks_per_sm<F>(), bases == nullptr);
+  lay.plan(n, limbs, c, sms, acc_blocks_per_sm<F>(dev), bases == nullptr);
   if ((uint64_t)n * lay.dp.W >= (1ull << 32)) {
     set_last_error("too many (point, window) entries for 32-bit offsets");
     return GM_ERR_ARG;
@@ -150,8 +154,8 @@ int msm_launch(cudaStream_t s, int dev, const uint4 *bases, const uint64_t *ref_
   auto *hk = (int32_t *)(ws + lay.o_hk);
   auto *tk = (int32_t *)(ws + lay.o_tk);
   auto *err = (uint32_t *)(ws + lay.o_err);
-  xyzz_t<F> *red[4];
-  for (int k = 0; k < 4; k++) red[k] = (xyzz_t<F> *)(ws + lay.o_red[k]);
+  xyzz_t<F> *red[3];
+  for (int k = 0; k < 3; k++) red[k] = (xyzz_t<F> *)(ws + lay.o_red[k]);
 
   profile_mark(s, "start");
   int launches = 0;
@@ -176,7 +180,7 @@ int msm_launch(cudaStream_t s, int dev, const uint4 *bases, const uint64_t *ref_
   GM_CHECK_LAUNCH("k_scatter");
   launches += 5;
   profile_mark(s, "sort");
-  k_accumulate<F><<<grid_for(lay.nthreads, 128), 128, 0, s>>>(bases, entries, offsets, lay.K, lay.nthreads, buckets,
+  k_accumulate<F><<<grid_for(lay.nthreads, ACC_THREADS), ACC_THREADS, acc_smem_bytes<F>(), s>>>(bases, entries, offsets, lay.K, lay.nthreads, buckets,
                                                                head, tail, hk, tk);
   GM_CHECK_LAUNCH("k_accumulate");
   launches++;
@@ -186,35 +190,40 @@ int msm_launch(cudaStream_t s, int dev, const uint4 *bases, const uint64_t *ref_
   launches++;
   profile_mark(s, "fixup");
 
-  // bucket reduction levels
+  // bucket reduction: per-segment shares, then a fan-in tree per window
   const int W = lay.dp.W;
-  int N = lay.dp.B;
-  int L = std::min(lay.L1, N);
-  int cur = 0;
   {
-    const int64_t th = (int64_t)W * ((N + L - 1) / L);
-    k_reduce_buckets<F><<<grid_for(th, 128), 128, 0, s>>>(buckets, offsets, W, lay.dp.B, L, red[0], red[1]);
-    GM_CHECK_LAUNCH("k_reduce_buckets");
+    const int64_t th = (int64_t)W * lay.nseg;
+    k_reduce_segments<F><<<grid_for(th, 128), 128, 0, s>>>(buckets, offsets, W, lay.dp.B, lay.L1, red[0]);
+    GM_CHECK_LAUNCH("k_reduce_segments");
     launches++;
   }
-  int ushift = 0;
-  for (int l = L; l > 1; l >>= 1) ushift++;
-  N = (N + L - 1) / L;
+  int N = lay.nseg;
+  xyzz_t<F> *src = red[0];
+  int pong = 1;
   while (N > 1) {
-    L = std::min(lay.Lk, N);
-    const int64_t th = (int64_t)W * ((N + L - 1) / L);
-    const int src = cur, dst = cur ^ 2;
-    k_reduce_level<F><<<grid_for(th, 128), 128, 0, s>>>(red[src], red[src + 1], W, N, L, ushift, red[dst], red[dst + 1]);
-    GM_CHECK_LAUNCH("k_reduce_level");
+    const int nout = (N + lay.FAN - 1) / lay.FAN;
+    xyzz_t<F> *dst = red[pong];
+    k_tree_sum<F><<<grid_for((int64_t)W * nout, 128), 128, 0, s>>>(src, W, N, lay.FAN, dst);
+    GM_CHECK_LAUNCH("k_tree_sum");
     launches++;
-    cur = dst;
-    for (int l = L; l > 1; l >>= 1) ushift++;
-    N = (N + L - 1) / L;
+    src = dst;
+    pong = pong == 1 ? 2 : 1;
+    N = nout;
   }
   profile_mark(s, "reduce");
-  k_combine<F><<<1, 1, 0, s>>>(red[cur], red[cur + 1], W, c, out_proj, nullptr);
-  GM_CHECK_LAUNCH("k_combine");
-  launches++;
+  // window combination: the serial Horner tail runs on the host (lower
+  // latency per product) unless the stream is being captured into a graph
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  GM_CHECK(cudaStreamIsCapturing(s, &cap));
+  if (cap == cudaStreamCaptureStatusNone && host_tail_enabled()) {
+    rc = enqueue_host_tail(s, F::LIMBS == NL ? 1 : 2, src, W, c, out_proj);
+    if (rc) return rc;
+  } else {
+    k_combine<F><<<1, 32, 0, s>>>(src, 1, W, c, out_proj);
+    GM_CHECK_LAUNCH("k_combine");
+    launches++;
+  }
   profile_mark(s, "combine");
   count_launches(launches);
   if (err_out) GM_CHECK(cudaMemcpyAsync(err_out, err, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));

@@ -44,6 +44,23 @@ struct Rec<Fp2> {
   static constexpr int U4 = 16;  // 256 B
 };
 
+// Arithmetic policy with the field product out of line (same data types).
+template <class F>
+struct OutOfLine;
+template <>
+struct OutOfLine<Fp> {
+  using type = FpOut;
+};
+template <>
+struct OutOfLine<Fp2> {
+  using type = Fp2Out;
+};
+
+template <class A, class B>
+GM_DEVI xyzz_t<A> as_xyzz(const xyzz_t<B> &p) {
+  return xyzz_t<A>{p.X, p.Y, p.ZZ, p.ZZZ};
+}
+
 template <class F>
 GM_DEVI uint32_t &limb_ref(typename F::T &a, int i);
 template <>
@@ -325,13 +342,38 @@ GM_DEVI int64_t bucket_of(const uint32_t *__restrict__ offsets, int64_t K, uint3
   return lo;
 }
 
+// Asynchronous 16-byte global -> shared copy (cp.async, L2 only).
+GM_DEVI void cp_async16(void *smem, const void *gmem) {
+  const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem));
+}
+GM_DEVI void cp_async_commit() { asm volatile("cp.async.commit_group;"); }
+GM_DEVI void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+constexpr int ACC_THREADS = 128;
 template <class F>
-__global__ void __launch_bounds__(128) k_accumulate(const uint4 *__restrict__ bases, const uint32_t *__restrict__ entries,
+constexpr int acc_smem_bytes() {
+  return 2 * (F::LIMBS / 2) * ACC_THREADS * 16;
+}
+
+// The base of the next entry is staged into shared memory with cp.async while
+// the current mixed addition runs, so the random 112/224-byte gather is off
+// the critical path.  Each thread owns two slots (double buffer); slots are
+// laid out chunk-major ([slot][chunk][thread]) so a warp's 16-byte accesses
+// hit consecutive banks.  Only the owning thread reads its slots, so no
+// block-level barrier is needed.
+template <class F>
+__global__ void __launch_bounds__(ACC_THREADS) k_accumulate(const uint4 *__restrict__ bases, const uint32_t *__restrict__ entries,
                                                     const uint32_t *__restrict__ offsets, int64_t K, int64_t nthreads,
                                                     xyzz_t<F> *__restrict__ buckets,
                                                     xyzz_t<F> *__restrict__ part_head, xyzz_t<F> *__restrict__ part_tail,
                                                     int32_t *__restrict__ head_key, int32_t *__restrict__ tail_key) {
   using T = typename F::T;
+  using FA = typename OutOfLine<F>::type;
+  constexpr int CH = F::LIMBS / 2;  // 16-byte chunks of x || y
+  extern __shared__ uint4 stage_mem[];  // [2][CH][ACC_THREADS], acc_smem_bytes<F>()
+  auto stage = reinterpret_cast<uint4(*)[CH][ACC_THREADS]>(stage_mem);
+  const int tid = threadIdx.x;
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nthreads) return;
   int32_t hk = -1, tk = -1;
@@ -346,24 +388,56 @@ __global__ void __launch_bounds__(128) k_accumulate(const uint4 *__restrict__ ba
     int64_t k = bucket_of(offsets, K, start);
     uint32_t bend = __ldg(offsets + k + 1);
     bool owns = __ldg(offsets + k) == start;
-    xyzz_t<F> acc;
+    xyzz_t<FA> acc;
     xyzz_set_inf(acc);
     uint32_t pos = start;
+    uint32_t e_cur = __ldg(entries + pos);
+    uint32_t e_nxt = (pos + 1 < end) ? __ldg(entries + pos + 1) : 0u;
+    {
+      const uint4 *src = bases + (size_t)(e_cur >> 1) * Rec<F>::U4;
+#pragma unroll
+      for (int q = 0; q < CH; q++) cp_async16(&stage[0][q][tid], src + q);
+      cp_async_commit();
+    }
+    int slot = 0;
     while (true) {
-      const uint32_t e = __ldg(entries + pos);
+      // prefetch the base of the next entry, and the entry after it
+      if (pos + 1 < end) {
+        const uint4 *src = bases + (size_t)(e_nxt >> 1) * Rec<F>::U4;
+#pragma unroll
+        for (int q = 0; q < CH; q++) cp_async16(&stage[slot ^ 1][q][tid], src + q);
+      }
+      cp_async_commit();
+      const uint32_t e_after = (pos + 2 < end) ? __ldg(entries + pos + 2) : 0u;
+      cp_async_wait_prev();
       T x, y;
-      load_base<F>(x, y, bases + (size_t)(e >> 1) * Rec<F>::U4);
-      if (e & 1u) y = F::neg(y);
-      xyzz_madd<F>(acc, x, y);
+#pragma unroll
+      for (int q = 0; q < CH; q++) {
+        const uint4 v = stage[slot][q][tid];
+        const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+          const int idx = 4 * q + e;
+          if (idx < F::LIMBS)
+            limb_ref<F>(x, idx) = w[e];
+          else
+            limb_ref<F>(y, idx - F::LIMBS) = w[e];
+        }
+      }
+      if (e_cur & 1u) y = F::neg(y);
+      xyzz_madd<FA>(acc, x, y);
       pos++;
+      slot ^= 1;
+      e_cur = e_nxt;
+      e_nxt = e_after;
       if (pos == bend || pos == end) {
         if (!owns) {
-          part_head[t] = acc;
+          part_head[t] = as_xyzz<F>(acc);
           hk = (int32_t)k;
         } else if (pos == bend) {
-          buckets[k] = acc;
+          buckets[k] = as_xyzz<F>(acc);
         } else {
-          part_tail[t] = acc;
+          part_tail[t] = as_xyzz<F>(acc);
           tk = (int32_t)k;
         }
         if (pos == end) break;
@@ -393,7 +467,8 @@ __global__ void __launch_bounds__(128) k_fixup(const uint32_t *__restrict__ offs
   const uint32_t M = __ldg(offsets + K);
   const uint64_t chunk64 = ((uint64_t)M + nthreads - 1) / nthreads;
   const uint32_t chunk = chunk64 > 0 ? (uint32_t)chunk64 : 1u;
-  xyzz_t<F> acc = part_tail[t];
+  using FA = typename OutOfLine<F>::type;
+  xyzz_t<FA> acc = as_xyzz<FA>(part_tail[t]);
   const uint64_t bend = __ldg(offsets + k + 1);
   int64_t t2 = t + 1;
   while (t2 < nthreads) {
@@ -401,102 +476,92 @@ __global__ void __launch_bounds__(128) k_fixup(const uint32_t *__restrict__ offs
       atomicOr(err, 1u);
       break;
     }
-    xyzz_t<F> h = part_head[t2];
-    xyzz_add_cold<F>(acc, h);
+    xyzz_add_cold<FA>(acc, as_xyzz<FA>(part_head[t2]));
     if ((uint64_t)(t2 + 1) * chunk >= bend) break;
     t2++;
   }
-  buckets[k] = acc;
+  buckets[k] = as_xyzz<F>(acc);
 }
 
 // ---------------------------------------------------------------------------
 // 6. bucket reduction: per window  S = sum_{j=0}^{B-1} (j+1) * V_j.
 //
-// Level input per window: N elements A_j (and, above level 1, carried partial
-// results R_j).  A thread takes a segment [s*L, s*L+L) and computes by a
-// running sum from the top
-//     ws = sum_j (j - s*L) * A_j,   a = sum_j A_j,   r = sum_j R_j,
-// and emits  R' = r + 2^ushift * ws,  A' = a.  With U = the product of the
-// segment lengths of the levels below,  sum_j j*V_j = sum R' + U*L * sum_s s*A'_s,
-// so the next level sees the same problem on N/L elements.  When one element
-// per window is left, S = R + A.
+// k_reduce_segments: one thread per segment [j0, j0+L) of a window computes,
+// by a running sum from the top, ws = sum (j - j0) V_j and a = sum V_j, then
+// its share of S directly:  ws + (j0 + 1) * a  (double-and-add by the small
+// integer j0 + 1).  The segment shares of a window are then added by a
+// fan-in tree (k_tree_sum).  Serial depth: 2L additions + log2(B) doublings
+// + log_fan(B/L) tree levels, with every stage spread over all segments.
 // ---------------------------------------------------------------------------
 template <class F>
-__global__ void __launch_bounds__(128) k_reduce_buckets(const xyzz_t<F> *__restrict__ buckets,
-                                                        const uint32_t *__restrict__ offsets, int W, int B, int L,
-                                                        xyzz_t<F> *__restrict__ R_out, xyzz_t<F> *__restrict__ A_out) {
+__global__ void __launch_bounds__(128) k_reduce_segments(const xyzz_t<F> *__restrict__ buckets,
+                                                         const uint32_t *__restrict__ offsets, int W, int B, int L,
+                                                         xyzz_t<F> *__restrict__ V_out) {
+  using FA = typename OutOfLine<F>::type;
   const int nseg = (B + L - 1) / L;
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (int64_t)W * nseg) return;
   const int w = (int)(t / nseg), s = (int)(t % nseg);
   const int64_t kb = (int64_t)w * B;
-  xyzz_t<F> acc, ws;
+  xyzz_t<FA> acc, ws;
   xyzz_set_inf(acc);
   xyzz_set_inf(ws);
   const int j0 = s * L, j1 = min(B, j0 + L);
   for (int j = j1 - 1; j >= j0; j--) {
-    if (__ldg(offsets + kb + j + 1) != __ldg(offsets + kb + j)) {
-      xyzz_t<F> v = buckets[kb + j];
-      xyzz_add_cold<F>(acc, v);
+    if (__ldg(offsets + kb + j + 1) != __ldg(offsets + kb + j)) xyzz_add<FA>(acc, as_xyzz<FA>(buckets[kb + j]));
+    if (j > j0) xyzz_add<FA>(ws, acc);
+  }
+  // ws += (j0 + 1) * acc, MSB-first double-and-add
+  const uint32_t mult = (uint32_t)j0 + 1u;
+  if (!xyzz_is_inf(acc)) {
+    xyzz_t<FA> m;
+    xyzz_set_inf(m);
+    for (int b = 31 - __clz(mult); b >= 0; b--) {
+      xyzz_dbl<FA>(m, m);
+      if ((mult >> b) & 1u) xyzz_add<FA>(m, acc);
     }
-    if (j > j0) xyzz_add_cold<F>(ws, acc);
+    xyzz_add<FA>(ws, m);
   }
-  R_out[t] = ws;
-  A_out[t] = acc;
+  V_out[t] = as_xyzz<F>(ws);
 }
 
+// out[g][i] = sum_{k < fan} in[g][i*fan + k]  (groups of N elements)
 template <class F>
-__global__ void __launch_bounds__(128) k_reduce_level(const xyzz_t<F> *__restrict__ R_in, const xyzz_t<F> *__restrict__ A_in,
-                                                      int W, int N, int L, int ushift, xyzz_t<F> *__restrict__ R_out,
-                                                      xyzz_t<F> *__restrict__ A_out) {
-  const int nseg = (N + L - 1) / L;
+__global__ void __launch_bounds__(128) k_tree_sum(const xyzz_t<F> *__restrict__ in, int groups, int N, int fan,
+                                                  xyzz_t<F> *__restrict__ out) {
+  using FA = typename OutOfLine<F>::type;
+  const int nout = (N + fan - 1) / fan;
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (int64_t)W * nseg) return;
-  const int w = (int)(t / nseg), s = (int)(t % nseg);
-  const int64_t kb = (int64_t)w * N;
-  xyzz_t<F> acc, ws, r;
-  xyzz_set_inf(acc);
-  xyzz_set_inf(ws);
-  xyzz_set_inf(r);
-  const int j0 = s * L, j1 = min(N, j0 + L);
-  for (int j = j1 - 1; j >= j0; j--) {
-    xyzz_t<F> a = A_in[kb + j];
-    xyzz_add_cold<F>(acc, a);
-    if (j > j0) xyzz_add_cold<F>(ws, acc);
-    xyzz_t<F> rr = R_in[kb + j];
-    xyzz_add_cold<F>(r, rr);
-  }
-  for (int k = 0; k < ushift; k++) xyzz_dbl_cold<F>(ws);
-  xyzz_add_cold<F>(r, ws);
-  R_out[t] = r;
-  A_out[t] = acc;
+  if (t >= (int64_t)groups * nout) return;
+  const int g = (int)(t / nout), i = (int)(t % nout);
+  const int64_t base = (int64_t)g * N + (int64_t)i * fan;
+  xyzz_t<FA> acc = as_xyzz<FA>(in[base]);
+  for (int k = 1; k < fan && i * fan + k < N; k++) xyzz_add<FA>(acc, as_xyzz<FA>(in[base + k]));
+  out[t] = as_xyzz<F>(acc);
 }
 
-// 7. Horner over windows; writes the homogeneous projective result in the
-// reference layout (X, Y, Z; u64 limbs; Montgomery form).
+// 7. Horner over windows on the device, one thread per MSM (used inside
+// CUDA-graph capture and for batches, where the host tail is not used);
+// writes the homogeneous projective result (X, Y, Z; u64 limbs; Montgomery).
 template <class F>
-__global__ void k_combine(const xyzz_t<F> *__restrict__ R, const xyzz_t<F> *__restrict__ A, int W, int c,
-                          uint64_t *__restrict__ out_proj, xyzz_t<F> *__restrict__ out_xyzz) {
-  if (blockIdx.x != 0 || threadIdx.x != 0) return;
-  xyzz_t<F> res;
+__global__ void k_combine(const xyzz_t<F> *__restrict__ S, int n_msm, int W, int c, uint64_t *__restrict__ out_proj) {
+  using FA = typename OutOfLine<F>::type;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_msm) return;
+  xyzz_t<FA> res;
   xyzz_set_inf(res);
   for (int w = W - 1; w >= 0; w--) {
     if (!xyzz_is_inf(res))
-      for (int k = 0; k < c; k++) xyzz_dbl_cold<F>(res);
-    xyzz_t<F> s = R[w];
-    xyzz_t<F> a = A[w];
-    xyzz_add_cold<F>(s, a);
-    xyzz_add_cold<F>(res, s);
+      for (int k = 0; k < c; k++) xyzz_dbl<FA>(res, res);
+    xyzz_add<FA>(res, as_xyzz<FA>(S[(int64_t)i * W + w]));
   }
-  if (out_xyzz) *out_xyzz = res;
-  if (out_proj) {
-    typename F::T X, Y, Z;
-    xyzz_to_proj<F>(X, Y, Z, res);
-    constexpr int H = F::LIMBS / 2;  // u64 words per coordinate
-    store_ref<F>(out_proj, X);
-    store_ref<F>(out_proj + H, Y);
-    store_ref<F>(out_proj + 2 * H, Z);
-  }
+  typename F::T X, Y, Z;
+  xyzz_to_proj<FA>(X, Y, Z, res);
+  constexpr int H = F::LIMBS / 2;  // u64 words per coordinate
+  uint64_t *o = out_proj + (int64_t)i * 3 * H;
+  store_ref<F>(o, X);
+  store_ref<F>(o + H, Y);
+  store_ref<F>(o + 2 * H, Z);
 }
 
 }  // namespace gm
