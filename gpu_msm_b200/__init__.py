@@ -58,7 +58,7 @@ C_API = [
     "gm_g1_to_montgomery_batch", "gm_g2_to_montgomery_batch",
     "gm_g1_generator_mul_batch", "gm_g2_generator_mul_batch", "gm_last_error",
     "gm_profile_enable", "gm_profile_collect", "gm_launch_count_reset", "gm_imad_probe",
-    "gm_g1_sum_projective", "gm_g2_sum_projective",
+    "gm_g1_sum_projective", "gm_g2_sum_projective", "gm_g1_msm_device_noalloc",
 ]
 
 
@@ -100,6 +100,7 @@ def lib() -> ctypes.CDLL:
         L.gm_profile_collect.argtypes = [ctypes.c_char_p, i32, vp, i32]
         L.gm_launch_count_reset.restype = i64
         L.gm_imad_probe.argtypes = [vp, u32, i32, vp, i64, vp]
+        L.gm_g1_msm_device_noalloc.argtypes = [vp, u32, vp, vp, vp, i32, i32]
         for name in ("gm_g1_sum_projective", "gm_g2_sum_projective"):
             getattr(L, name).argtypes = [vp, u32, vp, vp, i32]
         _lib = L
@@ -280,6 +281,28 @@ def msm_device(points, scalars, group: int = 1, window_bits: int = 0, out=None, 
     _check(fn(_stream_handle(stream), _dev_index(points), ctypes.c_void_p(out.data_ptr()),
               ctypes.c_void_p(points.data_ptr()), ctypes.c_void_p(scalars.data_ptr()), limbs, n, window_bits),
            "msm_device")
+    return out
+
+
+NOALLOC_MAX_POINTS = 4096
+
+
+def msm_device_noalloc(points, scalars, out=None, stream=None):
+    """G1 MSM through gm_g1_msm_device_noalloc, for callers that cannot
+    allocate device memory per call: the workspace is fixed in the library's
+    device image, so at most 4096 points per call.  Calls that overlap on the
+    GPU share that workspace and race; keep them on one stream."""
+    import torch
+    _require(points, G1_WORDS, "points")
+    n = points.shape[0]
+    _require(scalars, None, "scalars", rows=n)
+    if out is None:
+        out = torch.empty(G1P_WORDS, dtype=torch.int64, device=points.device)
+    if out.numel() < G1P_WORDS or out.dtype != torch.int64 or out.device != points.device:
+        raise ValueError("out: int64 tensor of the result size on the points' device")
+    _check(lib().gm_g1_msm_device_noalloc(_stream_handle(stream), _dev_index(points), ctypes.c_void_p(out.data_ptr()),
+                                          ctypes.c_void_p(points.data_ptr()), ctypes.c_void_p(scalars.data_ptr()),
+                                          scalars.shape[1], n), "msm_device_noalloc")
     return out
 
 

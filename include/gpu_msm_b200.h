@@ -120,6 +120,20 @@ int gm_g1_msm_device_c(gm_stream_t stream, uint32_t gpu_index, G1ProjectivePoint
 int gm_g2_msm_device_c(gm_stream_t stream, uint32_t gpu_index, G2ProjectivePoint *d_result, const G2Point *d_points,
                        const uint64_t *d_scalars, int scalar_limbs, int n, int window_bits);
 
+/* G1 MSM that allocates nothing.  No counterpart in the reference.  For
+ * callers that cannot allocate device memory per call: frameworks that hand
+ * almost all of HBM to their own caching allocator, and latency-critical code
+ * that must not take the implicit synchronisation of cudaMalloc/cudaFree.
+ * Same arguments and result as gm_g1_msm_device, but the workspace is a fixed
+ * 8 MiB array in the library's device image, reserved on every GPU that loads
+ * the library until the process exits.  Limit: n <= 4096 points and
+ * 1 <= scalar_limbs <= 8; larger requests return -1 without launching.  All
+ * calls share the array: calls that overlap on the GPU race, so order them on
+ * one stream.  The first call on a device looks up the array's address on
+ * that device; make it before any stream capture there. */
+int gm_g1_msm_device_noalloc(gm_stream_t stream, uint32_t gpu_index, G1ProjectivePoint *d_result,
+                             const G1Point *d_points, const uint64_t *d_scalars, int scalar_limbs, int n);
+
 /* Window width the cost model picks for an MSM of n points (group 1 or 2). */
 int gm_msm_default_window(int group, int64_t n, int scalar_limbs);
 
