@@ -362,7 +362,70 @@ def measure_extra(gm, wl, dev, imad_peak):
     ops2 = wl.msm_roofline_imad(n2, 2)
     out["g2_msm_2^18"] = {"points_per_s": n2 / t2, "ms": t2 * 1e3, "imad_frac": ops2 / t2 / imad_peak,
                           "window_bits": gm.default_window(2, n2, 5)}
+    del pts2, sc2_d
+    out["batched_512"] = measure_batched(gm, wl, dev)
     return out
+
+
+def measure_batched(gm, wl, dev, count=512, table_log2=16):
+    """512 independent G1 MSMs, sizes floor(2^U) with U ~ U[8, 16] (seeded),
+    each over a prefix of one resident 2^16-point table with its own scalars:
+    one batch plan (window widths per size class from the autotuner table)
+    captured in a CUDA graph, against 512 sequential plain launches."""
+    import torch
+    n_table = 1 << table_log2
+    logs = wl.make_base_logs(n_table, seed=7070)
+    pts = gm.generator_mul_batch(torch.from_numpy(logs.view(np.int64)).to(dev), group=1)
+    table = gm.ResidentBases(pts, group=1)
+    sizes = wl.mixed_sizes(count, 8, 16, seed=7)
+    total = int(sizes.sum())
+    sc = torch.from_numpy(wl.make_scalars(total, seed=7171).view(np.int64)).to(dev)
+    plan = gm.BatchPlan(table, sizes)
+    out = torch.empty((count, gm.G1P_WORDS), dtype=torch.int64, device=dev)
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        plan.run(sc, out=out)
+    torch.cuda.current_stream().wait_stream(s)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, capture_error_mode="thread_local"):
+        plan.run(sc, out=out)
+    g.replay()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 5
+    e0.record()
+    for _ in range(reps):
+        g.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    t_batch = e0.elapsed_time(e1) / reps / 1e3
+    # sequential plain launches over the same slices
+    rows = np.concatenate([[0], np.cumsum(sizes)])
+    seq_out = torch.empty((count, gm.G1P_WORDS), dtype=torch.int64, device=dev)
+    for i in range(4):
+        table.msm(sc[rows[i]:rows[i + 1]], offset=0, out=seq_out[i])
+    torch.cuda.synchronize()
+    e0.record()
+    for i in range(count):
+        table.msm(sc[rows[i]:rows[i + 1]], offset=0, window_bits=gm.tuned_window(1, int(sizes[i])), out=seq_out[i])
+    e1.record()
+    torch.cuda.synchronize()
+    t_seq = e0.elapsed_time(e1) / 1e3
+    # canonical equality of every output (projective forms may differ)
+    a = gm.to_numpy_proj(out, 1)
+    b_ = gm.to_numpy_proj(seq_out, 1)
+    same = all(np.array_equal(gm.projective_to_affine(a[i:i + 1], 1)["x"], gm.projective_to_affine(b_[i:i + 1], 1)["x"])
+               for i in range(0, count, 37))
+    res = {"count": count, "points": total, "classes": plan.classes(),
+           "batched_points_per_s": total / t_batch, "batched_ms": t_batch * 1e3,
+           "sequential_points_per_s": total / t_seq, "sequential_ms": t_seq * 1e3,
+           "speedup": t_seq / t_batch, "sampled_outputs_equal": same, "graph": "cuda graph replay"}
+    del g
+    plan.close()
+    table.close()
+    return res
 
 
 def main():

@@ -59,6 +59,8 @@ C_API = [
     "gm_g1_generator_mul_batch", "gm_g2_generator_mul_batch", "gm_last_error",
     "gm_profile_enable", "gm_profile_collect", "gm_launch_count_reset", "gm_imad_probe",
     "gm_g1_sum_projective", "gm_g2_sum_projective", "gm_g1_msm_device_noalloc",
+    "gm_bases_create", "gm_bases_destroy", "gm_bases_count", "gm_msm_resident", "gm_batch_plan_create",
+    "gm_batch_plan_run", "gm_batch_plan_destroy", "gm_batch_plan_bytes", "gm_batch_plan_classes",
 ]
 
 
@@ -101,6 +103,17 @@ def lib() -> ctypes.CDLL:
         L.gm_launch_count_reset.restype = i64
         L.gm_imad_probe.argtypes = [vp, u32, i32, vp, i64, vp]
         L.gm_g1_msm_device_noalloc.argtypes = [vp, u32, vp, vp, vp, i32, i32]
+        L.gm_bases_create.argtypes = [u32, i32, vp, i64, i32, vp]
+        L.gm_bases_destroy.argtypes = [vp]
+        L.gm_bases_count.argtypes = [vp]
+        L.gm_bases_count.restype = i64
+        L.gm_msm_resident.argtypes = [vp, vp, i64, i32, vp, i32, vp, i32]
+        L.gm_batch_plan_create.argtypes = [vp, i32, i32, vp, vp, vp, vp]
+        L.gm_batch_plan_run.argtypes = [vp, vp, vp, vp]
+        L.gm_batch_plan_destroy.argtypes = [vp]
+        L.gm_batch_plan_bytes.argtypes = [vp]
+        L.gm_batch_plan_bytes.restype = i64
+        L.gm_batch_plan_classes.argtypes = [vp, vp, vp, i32]
         for name in ("gm_g1_sum_projective", "gm_g2_sum_projective"):
             getattr(L, name).argtypes = [vp, u32, vp, vp, i32]
         _lib = L
@@ -405,3 +418,134 @@ def imad_probe(iters: int, sink, stream=None) -> int:
     _check(lib().gm_imad_probe(_stream_handle(stream), _dev_index(sink), iters, ctypes.c_void_p(sink.data_ptr()),
                                sink.numel(), ctypes.byref(cnt)), "imad_probe")
     return cnt.value
+
+
+# ---------------------------------------------------------------------------
+# resident base tables and batched MSMs
+# ---------------------------------------------------------------------------
+
+class ResidentBases:
+    """A base table packed once on the device (``gm_bases_create``).
+
+    points: int64 CUDA tensor (n, 15) [G1Point] or (n, 29) [G2Point] in the
+    reference layout; Montgomery form unless montgomery=False."""
+
+    def __init__(self, points, group: int = 1, montgomery: bool = True):
+        _require(points, G1_WORDS if group == 1 else G2_WORDS, "points")
+        self.group = group
+        self.n = points.shape[0]
+        self.device = points.device
+        h = ctypes.c_void_p()
+        _check(lib().gm_bases_create(_dev_index(points), group, ctypes.c_void_p(points.data_ptr()), self.n,
+                                     1 if montgomery else 0, ctypes.byref(h)), "gm_bases_create")
+        self.handle = h
+
+    def msm(self, scalars, offset: int = 0, n: int = None, window_bits: int = 0, out=None, stream=None):
+        """Asynchronous MSM over entries [offset, offset + n)."""
+        import torch
+        n = scalars.shape[0] if n is None else n
+        _require(scalars, None, "scalars", rows=n)
+        if offset < 0 or offset + n > self.n:
+            raise ValueError("range outside the base table")
+        words = G1P_WORDS if self.group == 1 else G2P_WORDS
+        if out is None:
+            out = torch.empty(words, dtype=torch.int64, device=self.device)
+        _check(lib().gm_msm_resident(_stream_handle(stream), self.handle, offset, n, ctypes.c_void_p(scalars.data_ptr()),
+                                     scalars.shape[1], ctypes.c_void_p(out.data_ptr()), window_bits),
+               "gm_msm_resident")
+        return out
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().gm_bases_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_WINDOW_TABLE = None
+
+
+def window_table() -> dict:
+    """The autotuner's table (gpu_msm_b200/window_table.json), or {}."""
+    global _WINDOW_TABLE
+    if _WINDOW_TABLE is None:
+        import json
+        path = os.path.join(_HERE, "window_table.json")
+        try:
+            with open(path) as f:
+                _WINDOW_TABLE = json.load(f)
+        except (OSError, ValueError):
+            _WINDOW_TABLE = {}
+    return _WINDOW_TABLE
+
+
+def tuned_window(group: int, n: int, scalar_limbs: int = 5) -> int:
+    """Window width for an MSM of n points: the autotuned value for its size
+    class floor(log2 n) when tuned, else the library's cost model."""
+    tab = window_table().get(f"g{group}", {})
+    e = max(0, int(n).bit_length() - 1)
+    if str(e) in tab:
+        return int(tab[str(e)])
+    return default_window(group, n, scalar_limbs)
+
+
+class BatchPlan:
+    """A fixed batch of MSMs over a resident table (``gm_batch_plan_*``).
+
+    sizes[i] points for MSM i starting at table entry base_offsets[i];
+    window_bits[i] (0: cost model).  ``run`` enqueues the whole batch on the
+    current (or given) stream; it only launches kernels, so it can be captured
+    in a CUDA graph and replayed with new scalars in the same tensor."""
+
+    def __init__(self, bases: ResidentBases, sizes, base_offsets=None, window_bits=None, scalar_limbs: int = 5):
+        self.bases = bases
+        self.sizes = np.ascontiguousarray(sizes, dtype=np.int64)
+        self.count = len(self.sizes)
+        self.total = int(self.sizes.sum())
+        self.limbs = scalar_limbs
+        offs = None if base_offsets is None else np.ascontiguousarray(base_offsets, dtype=np.int64)
+        if window_bits is None:
+            window_bits = [tuned_window(bases.group, int(s), scalar_limbs) for s in self.sizes]
+        wins = np.ascontiguousarray(window_bits, dtype=np.int32)
+        h = ctypes.c_void_p()
+        _check(lib().gm_batch_plan_create(bases.handle, scalar_limbs, self.count, _p(self.sizes),
+                                          None if offs is None else _p(offs), None if wins is None else _p(wins),
+                                          ctypes.byref(h)), "gm_batch_plan_create")
+        self.handle = h
+        self._keep = (offs, wins)
+
+    @property
+    def workspace_bytes(self) -> int:
+        return int(lib().gm_batch_plan_bytes(self.handle))
+
+    def classes(self):
+        w = np.zeros(64, dtype=np.int32)
+        c = np.zeros(64, dtype=np.int32)
+        k = lib().gm_batch_plan_classes(self.handle, _p(w), _p(c), 64)
+        return list(zip(w[:k].tolist(), c[:k].tolist()))
+
+    def run(self, scalars, out=None, stream=None):
+        import torch
+        _require(scalars, self.limbs, "scalars", rows=self.total)
+        words = G1P_WORDS if self.bases.group == 1 else G2P_WORDS
+        if out is None:
+            out = torch.empty((self.count, words), dtype=torch.int64, device=scalars.device)
+        _check(lib().gm_batch_plan_run(self.handle, _stream_handle(stream), ctypes.c_void_p(scalars.data_ptr()),
+                                       ctypes.c_void_p(out.data_ptr())), "gm_batch_plan_run")
+        return out
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().gm_batch_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

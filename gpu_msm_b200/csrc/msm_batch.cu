@@ -1,0 +1,243 @@
+// C-ABI of resident base tables and batched MSM plans (include/gpu_msm_b200.h,
+// part 2).  The reference has neither: every reference MSM call copies its
+// bases in and converts them again (rust-api/src/c_wrapper.cu:64-172).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <new>
+#include <vector>
+
+#include "../../include/gpu_msm_b200.h"
+#include "msm_batch.cuh"
+
+namespace gm {
+// heavy templates are instantiated once, in msm_g1.cu / msm_g2.cu
+extern template int msm_launch<Fp>(cudaStream_t, int, const uint4 *, const uint64_t *, int, const uint64_t *, int,
+                                   int64_t, uint64_t *, int, uint32_t *);
+extern template int msm_launch<Fp2>(cudaStream_t, int, const uint4 *, const uint64_t *, int, const uint64_t *, int,
+                                    int64_t, uint64_t *, int, uint32_t *);
+extern template int batch_layouts<Fp>(BatchPlan &, int);
+extern template int batch_layouts<Fp2>(BatchPlan &, int);
+extern template int batch_run<Fp>(const BatchPlan &, cudaStream_t, const uint64_t *, uint64_t *);
+extern template int batch_run<Fp2>(const BatchPlan &, cudaStream_t, const uint64_t *, uint64_t *);
+}  // namespace gm
+
+struct gm_bases {
+  int group = 1;
+  int dev = 0;
+  int64_t n = 0;
+  uint4 *packed = nullptr;  // owned, Rec<F>::U4 uint4 per point
+};
+
+struct gm_batch_plan {
+  gm::BatchPlan plan;
+};
+
+namespace {
+
+void free_plan(gm_batch_plan *p) {
+  for (auto &cp : p->plan.classes) {
+    if (cp.ws) cudaFree(cp.ws);
+    if (cp.desc) cudaFree(cp.desc);
+    if (cp.stream) cudaStreamDestroy(cp.stream);
+    if (cp.done) cudaEventDestroy(cp.done);
+  }
+  if (p->plan.fork) cudaEventDestroy(p->plan.fork);
+  delete p;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gm_bases_create(uint32_t gpu_index, int group, const void *d_points, int64_t n, int points_montgomery,
+                    gm_bases **out) {
+  if (out == nullptr || (group != 1 && group != 2) || n <= 0 || n >= (int64_t(1) << 31) || d_points == nullptr)
+    return gm::GM_ERR_ARG;
+  int rc = gm::select_device(gpu_index);
+  if (rc) return rc;
+  auto *b = new (std::nothrow) gm_bases;
+  if (!b) return gm::GM_ERR_ALLOC;
+  b->group = group;
+  b->dev = (int)gpu_index;
+  b->n = n;
+  const int u4 = group == 1 ? gm::Rec<gm::Fp>::U4 : gm::Rec<gm::Fp2>::U4;
+  cudaError_t e = cudaMalloc(&b->packed, (size_t)n * u4 * sizeof(uint4));
+  if (e != cudaSuccess) {
+    delete b;
+    gm::record_error(e, "cudaMalloc(bases)");
+    return gm::GM_ERR_ALLOC;
+  }
+  const unsigned grid = (unsigned)((n + 255) / 256);
+  const int to_mont = points_montgomery ? 0 : 1;
+  if (group == 1)
+    gm::k_pack_ref<gm::Fp><<<grid, 256>>>(b->packed, (const uint64_t *)d_points, n, 15, to_mont);
+  else
+    gm::k_pack_ref<gm::Fp2><<<grid, 256>>>(b->packed, (const uint64_t *)d_points, n, 29, to_mont);
+  gm::count_launches(1);
+  e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) {
+    cudaFree(b->packed);
+    delete b;
+    return gm::record_error(e, "k_pack_ref(bases)");
+  }
+  *out = b;
+  return gm::GM_OK;
+}
+
+int gm_bases_destroy(gm_bases *b) {
+  if (!b) return gm::GM_OK;
+  cudaSetDevice(b->dev);
+  cudaFree(b->packed);
+  delete b;
+  return gm::GM_OK;
+}
+
+int64_t gm_bases_count(const gm_bases *b) { return b ? b->n : 0; }
+
+int gm_msm_resident(gm_stream_t stream, const gm_bases *b, int64_t base_offset, int n, const uint64_t *d_scalars,
+                    int scalar_limbs, void *d_result, int window_bits) {
+  if (!b || d_result == nullptr || n < 0 || base_offset < 0 || base_offset + n > b->n ||
+      (n > 0 && d_scalars == nullptr))
+    return gm::GM_ERR_ARG;
+  int rc = gm::select_device((uint32_t)b->dev);
+  if (rc) return rc;
+  if (b->group == 1)
+    return gm::msm_launch<gm::Fp>((cudaStream_t)stream, b->dev, b->packed + base_offset * gm::Rec<gm::Fp>::U4, nullptr,
+                                  0, d_scalars, scalar_limbs, n, (uint64_t *)d_result, window_bits, nullptr);
+  return gm::msm_launch<gm::Fp2>((cudaStream_t)stream, b->dev, b->packed + base_offset * gm::Rec<gm::Fp2>::U4, nullptr,
+                                 0, d_scalars, scalar_limbs, n, (uint64_t *)d_result, window_bits, nullptr);
+}
+
+int gm_batch_plan_create(const gm_bases *b, int scalar_limbs, int count, const int64_t *sizes,
+                         const int64_t *base_offsets, const int32_t *window_bits, gm_batch_plan **out) {
+  if (!b || !out || count <= 0 || !sizes || scalar_limbs < 1 || scalar_limbs > gm::MAX_SCALAR_LIMBS)
+    return gm::GM_ERR_ARG;
+  int rc = gm::select_device((uint32_t)b->dev);
+  if (rc) return rc;
+  // validate and group MSMs by window width
+  std::map<int, std::vector<int>> by_c;
+  std::vector<int64_t> sc_row(count + 1, 0);
+  for (int i = 0; i < count; i++) {
+    const int64_t off = base_offsets ? base_offsets[i] : 0;
+    if (sizes[i] <= 0 || off < 0 || off + sizes[i] > b->n) {
+      gm::set_last_error("batch MSM outside the base table or empty");
+      return gm::GM_ERR_ARG;
+    }
+    sc_row[i + 1] = sc_row[i] + sizes[i];
+    int c = window_bits && window_bits[i] > 0 ? window_bits[i] : gm::default_window(b->group, sizes[i], scalar_limbs);
+    if (c < 2 || c > 20) {
+      gm::set_last_error("window width out of range");
+      return gm::GM_ERR_ARG;
+    }
+    by_c[c].push_back(i);
+  }
+  auto *p = new (std::nothrow) gm_batch_plan;
+  if (!p) return gm::GM_ERR_ALLOC;
+  gm::BatchPlan &plan = p->plan;
+  plan.group = b->group;
+  plan.dev = b->dev;
+  plan.limbs = scalar_limbs;
+  plan.count = count;
+  plan.bases = b->packed;
+  plan.n_bases = b->n;
+  for (auto &kv : by_c) {
+    gm::BatchClassPlan cp;
+    cp.c = kv.first;
+    cp.count = (int)kv.second.size();
+    int64_t P = 0;
+    for (int i : kv.second) P += sizes[i];
+    cp.P = P;
+    plan.classes.push_back(cp);
+  }
+  int sms = 0;
+  rc = gm::device_sm_count(b->dev, &sms);
+  if (rc) {
+    free_plan(p);
+    return rc;
+  }
+  if (b->group == 1)
+    gm::batch_layouts<gm::Fp>(plan, sms);
+  else
+    gm::batch_layouts<gm::Fp2>(plan, sms);
+  size_t ci = 0;
+  for (auto &kv : by_c) {
+    gm::BatchClassPlan &cp = plan.classes[ci++];
+    if ((uint64_t)cp.P * cp.dp.W >= (1ull << 32)) {
+      free_plan(p);
+      gm::set_last_error("batch class too large for 32-bit entry offsets");
+      return gm::GM_ERR_ARG;
+    }
+    // descriptors: point_start[count+1] | base_off[count] | sc_off[count] | out_index[count] (int32)
+    std::vector<int64_t> d64(3 * (size_t)cp.count + 1);
+    std::vector<int32_t> idx(cp.count);
+    int64_t acc = 0;
+    for (int k = 0; k < cp.count; k++) {
+      const int i = kv.second[k];
+      d64[k] = acc;
+      acc += sizes[i];
+      d64[cp.count + 1 + k] = base_offsets ? base_offsets[i] : 0;
+      d64[2 * cp.count + 1 + k] = sc_row[i];
+      idx[k] = i;
+    }
+    d64[cp.count] = acc;
+    const size_t desc_bytes = d64.size() * sizeof(int64_t) + idx.size() * sizeof(int32_t);
+    cudaError_t e = cudaMalloc(&cp.desc, desc_bytes);
+    if (e == cudaSuccess) e = cudaMemcpy(cp.desc, d64.data(), d64.size() * sizeof(int64_t), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(cp.desc + d64.size() * sizeof(int64_t), idx.data(), idx.size() * sizeof(int32_t),
+                     cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMalloc(&cp.ws, cp.ws_bytes);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&cp.stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&cp.done, cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+      free_plan(p);
+      gm::record_error(e, "batch plan allocation");
+      return gm::GM_ERR_ALLOC;
+    }
+    plan.bytes += cp.ws_bytes + desc_bytes;
+  }
+  cudaError_t e = cudaEventCreateWithFlags(&plan.fork, cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    free_plan(p);
+    return gm::record_error(e, "cudaEventCreate");
+  }
+  *out = p;
+  return gm::GM_OK;
+}
+
+int gm_batch_plan_run(gm_batch_plan *p, gm_stream_t stream, const uint64_t *d_scalars, void *d_results) {
+  if (!p || !d_scalars || !d_results) return gm::GM_ERR_ARG;
+  int rc = gm::select_device((uint32_t)p->plan.dev);
+  if (rc) return rc;
+  if (p->plan.group == 1) return gm::batch_run<gm::Fp>(p->plan, (cudaStream_t)stream, d_scalars, (uint64_t *)d_results);
+  return gm::batch_run<gm::Fp2>(p->plan, (cudaStream_t)stream, d_scalars, (uint64_t *)d_results);
+}
+
+int gm_batch_plan_destroy(gm_batch_plan *p) {
+  if (!p) return gm::GM_OK;
+  cudaSetDevice(p->plan.dev);
+  cudaDeviceSynchronize();
+  free_plan(p);
+  return gm::GM_OK;
+}
+
+int64_t gm_batch_plan_bytes(const gm_batch_plan *p) { return p ? (int64_t)p->plan.bytes : 0; }
+
+int gm_batch_plan_classes(const gm_batch_plan *p, int32_t *window_bits, int32_t *counts, int max) {
+  if (!p) return 0;
+  int k = 0;
+  for (const auto &cp : p->plan.classes) {
+    if (k < max) {
+      if (window_bits) window_bits[k] = cp.c;
+      if (counts) counts[k] = cp.count;
+    }
+    k++;
+  }
+  return k;
+}
+
+}  // extern "C"

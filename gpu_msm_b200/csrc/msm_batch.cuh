@@ -1,0 +1,165 @@
+// Batched MSM engine: many independent MSMs of uneven size over one resident
+// base table, executed as one flattened pipeline per window-width class.
+//
+// A plan fixes the batch's shape (sizes, base offsets, window width per MSM),
+// groups the MSMs into classes of equal window width, uploads the per-MSM
+// descriptors and allocates every workspace once.  Running the plan only
+// enqueues kernels and memsets: each class on its own stream, forked from and
+// joined back to the caller's stream with events, so a run can be captured
+// into a CUDA graph and replayed with new scalars in the same buffer.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "msm_host.cuh"
+
+namespace gm {
+
+struct BatchClassPlan {
+  int c = 0;
+  DigitParams dp{};
+  int count = 0;        // MSMs in this class
+  int64_t P = 0;        // points in this class
+  int64_t K = 0, nb = 0, nthreads = 0;
+  int L1 = 8, FAN = 4, nseg = 0;
+  size_t o_counts = 0, o_offsets = 0, o_bsum = 0, o_entries = 0, o_buckets = 0, o_head = 0, o_tail = 0, o_hk = 0,
+         o_tk = 0, o_red[3] = {0, 0, 0}, o_err = 0;
+  size_t ws_bytes = 0;
+  char *ws = nullptr;       // workspace (owned)
+  char *desc = nullptr;     // point_start | base_off | sc_off | out_index (owned)
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;
+};
+
+struct BatchPlan {
+  int group = 1, dev = 0, limbs = 1, count = 0;
+  const uint4 *bases = nullptr;
+  int64_t n_bases = 0;
+  std::vector<BatchClassPlan> classes;
+  cudaEvent_t fork = nullptr;
+  size_t bytes = 0;
+};
+
+// Workspace layout of one class (same parts as a single MSM, K over all the
+// class's MSMs, no base packing).
+template <class F>
+void batch_class_layout(BatchClassPlan &cp, int limbs, int sms, int dev) {
+  cp.dp.c = cp.c;
+  cp.dp.W = windows_for(cp.c, limbs);
+  cp.dp.B = 1 << (cp.c - 1);
+  cp.dp.limbs = limbs;
+  cp.K = (int64_t)cp.count * cp.dp.W * cp.dp.B;
+  cp.nb = (cp.K + SCAN_TILE - 1) / SCAN_TILE;
+  cp.nthreads = (int64_t)sms * acc_blocks_per_sm<F>(dev) * ACC_THREADS;
+  const int64_t max_entries = cp.P * cp.dp.W;
+  if (cp.nthreads > max_entries) cp.nthreads = std::max<int64_t>(1, (max_entries + 127) / 128 * 128);
+  cp.L1 = std::min(8, cp.dp.B);
+  cp.nseg = (cp.dp.B + cp.L1 - 1) / cp.L1;
+  const int64_t red = (int64_t)cp.count * cp.dp.W * cp.nseg;
+  Carve cv;
+  cp.o_counts = cv.take<uint32_t>(cp.K);
+  cp.o_offsets = cv.take<uint32_t>(cp.K + 1);
+  cp.o_bsum = cv.take<uint32_t>(cp.nb);
+  cp.o_entries = cv.take<uint32_t>((size_t)std::max<int64_t>(1, max_entries));
+  cp.o_buckets = cv.take<xyzz_t<F>>(cp.K);
+  cp.o_head = cv.take<xyzz_t<F>>(cp.nthreads);
+  cp.o_tail = cv.take<xyzz_t<F>>(cp.nthreads);
+  cp.o_hk = cv.take<int32_t>(cp.nthreads);
+  cp.o_tk = cv.take<int32_t>(cp.nthreads);
+  cp.o_red[0] = cv.take<xyzz_t<F>>(red);
+  cp.o_red[1] = cv.take<xyzz_t<F>>((red + cp.FAN - 1) / cp.FAN + (int64_t)cp.count * cp.dp.W);
+  cp.o_red[2] = cv.take<xyzz_t<F>>((red + cp.FAN - 1) / cp.FAN + (int64_t)cp.count * cp.dp.W);
+  cp.o_err = cv.take<uint32_t>(4);
+  cp.ws_bytes = cv.off;
+}
+
+// Enqueue one class's pipeline on `s`.
+template <class F>
+int batch_class_run(const BatchPlan &plan, const BatchClassPlan &cp, cudaStream_t s, const uint64_t *scalars,
+                    uint64_t *results) {
+  if (cp.count == 0) return GM_OK;
+  char *ws = cp.ws;
+  auto *counts = (uint32_t *)(ws + cp.o_counts);
+  auto *offsets = (uint32_t *)(ws + cp.o_offsets);
+  auto *bsum = (uint32_t *)(ws + cp.o_bsum);
+  auto *entries = (uint32_t *)(ws + cp.o_entries);
+  auto *buckets = (xyzz_t<F> *)(ws + cp.o_buckets);
+  auto *head = (xyzz_t<F> *)(ws + cp.o_head);
+  auto *tail = (xyzz_t<F> *)(ws + cp.o_tail);
+  auto *hk = (int32_t *)(ws + cp.o_hk);
+  auto *tk = (int32_t *)(ws + cp.o_tk);
+  auto *err = (uint32_t *)(ws + cp.o_err);
+  xyzz_t<F> *red[3];
+  for (int k = 0; k < 3; k++) red[k] = (xyzz_t<F> *)(ws + cp.o_red[k]);
+  MultiDesc md;
+  md.point_start = (const int64_t *)cp.desc;
+  md.base_off = md.point_start + cp.count + 1;
+  md.sc_off = md.base_off + cp.count;
+  md.count = cp.count;
+  const int32_t *out_index = (const int32_t *)(md.sc_off + cp.count);
+
+  int launches = 0;
+  GM_CHECK(cudaMemsetAsync(counts, 0, cp.K * sizeof(uint32_t), s));
+  GM_CHECK(cudaMemsetAsync(err, 0, sizeof(uint32_t), s));
+  k_count_multi<<<grid_for(cp.P, 256), 256, 0, s>>>(scalars, plan.bases, Rec<F>::U4, F::LIMBS, cp.P, md, cp.dp,
+                                                    counts);
+  GM_CHECK_LAUNCH("k_count_multi");
+  k_scan_blocksum<<<(unsigned)cp.nb, SCAN_THREADS, 0, s>>>(counts, cp.K, bsum);
+  k_scan_top<<<1, SCAN_THREADS, 0, s>>>(bsum, (int)cp.nb);
+  k_scan_final<<<(unsigned)cp.nb, SCAN_THREADS, 0, s>>>(counts, cp.K, bsum, offsets);
+  GM_CHECK_LAUNCH("k_scan");
+  k_scatter_multi<<<grid_for(cp.P, 256), 256, 0, s>>>(scalars, plan.bases, Rec<F>::U4, F::LIMBS, cp.P, md, cp.dp,
+                                                      offsets, counts, entries);
+  GM_CHECK_LAUNCH("k_scatter_multi");
+  launches += 5;
+  k_accumulate<F><<<grid_for(cp.nthreads, ACC_THREADS), ACC_THREADS, acc_smem_bytes<F>(), s>>>(
+      plan.bases, entries, offsets, cp.K, cp.nthreads, buckets, head, tail, hk, tk);
+  GM_CHECK_LAUNCH("k_accumulate");
+  k_fixup<F><<<grid_for(cp.nthreads, 128), 128, 0, s>>>(offsets, cp.K, cp.nthreads, buckets, head, tail, hk, tk, err);
+  GM_CHECK_LAUNCH("k_fixup");
+  const int Wtot = cp.count * cp.dp.W;
+  k_reduce_segments<F><<<grid_for((int64_t)Wtot * cp.nseg, 128), 128, 0, s>>>(buckets, offsets, Wtot, cp.dp.B, cp.L1,
+                                                                             red[0]);
+  GM_CHECK_LAUNCH("k_reduce_segments");
+  launches += 3;
+  int N = cp.nseg, pong = 1;
+  xyzz_t<F> *src = red[0];
+  while (N > 1) {
+    const int nout = (N + cp.FAN - 1) / cp.FAN;
+    k_tree_sum<F><<<grid_for((int64_t)Wtot * nout, 128), 128, 0, s>>>(src, Wtot, N, cp.FAN, red[pong]);
+    GM_CHECK_LAUNCH("k_tree_sum");
+    launches++;
+    src = red[pong];
+    pong = pong == 1 ? 2 : 1;
+    N = nout;
+  }
+  k_combine_indexed<F><<<grid_for(cp.count, 32), 32, 0, s>>>(src, cp.count, cp.dp.W, cp.c, out_index, results);
+  GM_CHECK_LAUNCH("k_combine_indexed");
+  launches++;
+  count_launches(launches);
+  return GM_OK;
+}
+
+template <class F>
+int batch_layouts(BatchPlan &plan, int sms) {
+  for (auto &cp : plan.classes) batch_class_layout<F>(cp, plan.limbs, sms, plan.dev);
+  return GM_OK;
+}
+
+// Fork the classes onto their streams and join them back into `s`.
+template <class F>
+int batch_run(const BatchPlan &plan, cudaStream_t s, const uint64_t *scalars, uint64_t *results) {
+  if (plan.classes.size() == 1) return batch_class_run<F>(plan, plan.classes[0], s, scalars, results);
+  GM_CHECK(cudaEventRecord(plan.fork, s));
+  for (const auto &cp : plan.classes) {
+    GM_CHECK(cudaStreamWaitEvent(cp.stream, plan.fork, 0));
+    const int rc = batch_class_run<F>(plan, cp, cp.stream, scalars, results);
+    if (rc) return rc;
+    GM_CHECK(cudaEventRecord(cp.done, cp.stream));
+    GM_CHECK(cudaStreamWaitEvent(s, cp.done, 0));
+  }
+  return GM_OK;
+}
+
+}  // namespace gm

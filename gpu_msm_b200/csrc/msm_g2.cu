@@ -1,7 +1,9 @@
 // G2 instantiation of the MSM launch sequence.
-#include "msm_host.cuh"
+#include "msm_batch.cuh"
 
 namespace gm {
 template int msm_launch<Fp2>(cudaStream_t, int, const uint4 *, const uint64_t *, int, const uint64_t *, int, int64_t,
                              uint64_t *, int, uint32_t *);
+template int batch_layouts<Fp2>(BatchPlan &, int);
+template int batch_run<Fp2>(const BatchPlan &, cudaStream_t, const uint64_t *, uint64_t *);
 }  // namespace gm

@@ -239,6 +239,63 @@ static __global__ void k_scatter(const uint64_t *__restrict__ scalars, const uin
   });
 }
 
+// Many MSMs in one pipeline (batched mode).  MSM i owns the flattened point
+// ids [point_start[i], point_start[i+1]); its j-th point uses base record
+// base_off[i] + j of the shared table and scalar row sc_off[i] + j.  Its
+// bucket keys are i*W*B + w*B + |d|-1, so one counting sort, one
+// accumulation and one reduction serve every MSM of the batch.
+struct MultiDesc {
+  const int64_t *point_start;  // [count + 1]
+  const int64_t *base_off;     // [count]
+  const int64_t *sc_off;       // [count]
+  int count;
+};
+
+GM_DEVI int msm_of(const int64_t *__restrict__ ps, int count, int64_t p) {
+  int lo = 0, hi = count;  // ps[lo] <= p < ps[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(ps + mid) <= p)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+static __global__ void k_count_multi(const uint64_t *__restrict__ scalars, const uint4 *__restrict__ bases,
+                                     int rec_u4, int field_limbs, int64_t P, MultiDesc md, DigitParams dp,
+                                     uint32_t *__restrict__ counts) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P) return;
+  const int i = msm_of(md.point_start, md.count, p);
+  const int64_t j = p - __ldg(md.point_start + i);
+  const int64_t bi = __ldg(md.base_off + i) + j;
+  if (base_is_inf(bases + bi * rec_u4, rec_u4, field_limbs)) return;
+  const int64_t kbase = (int64_t)i * dp.W * dp.B;
+  for_each_digit(scalars + (__ldg(md.sc_off + i) + j) * dp.limbs, dp, [&](int w, int d) {
+    atomicAdd(&counts[kbase + (int64_t)w * dp.B + (d < 0 ? -d : d) - 1], 1u);
+  });
+}
+
+static __global__ void k_scatter_multi(const uint64_t *__restrict__ scalars, const uint4 *__restrict__ bases,
+                                       int rec_u4, int field_limbs, int64_t P, MultiDesc md, DigitParams dp,
+                                       const uint32_t *__restrict__ offsets, uint32_t *__restrict__ counts,
+                                       uint32_t *__restrict__ entries) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P) return;
+  const int i = msm_of(md.point_start, md.count, p);
+  const int64_t j = p - __ldg(md.point_start + i);
+  const int64_t bi = __ldg(md.base_off + i) + j;
+  if (base_is_inf(bases + bi * rec_u4, rec_u4, field_limbs)) return;
+  const int64_t kbase = (int64_t)i * dp.W * dp.B;
+  for_each_digit(scalars + (__ldg(md.sc_off + i) + j) * dp.limbs, dp, [&](int w, int d) {
+    const int64_t key = kbase + (int64_t)w * dp.B + (d < 0 ? -d : d) - 1;
+    const uint32_t rank = atomicSub(&counts[key], 1u) - 1u;
+    entries[offsets[key] + rank] = ((uint32_t)bi << 1) | (d < 0 ? 1u : 0u);
+  });
+}
+
 // ---------------------------------------------------------------------------
 // 2. exclusive scan (three kernels, 1024 elements per block)
 // ---------------------------------------------------------------------------
@@ -559,6 +616,29 @@ __global__ void k_combine(const xyzz_t<F> *__restrict__ S, int n_msm, int W, int
   xyzz_to_proj<FA>(X, Y, Z, res);
   constexpr int H = F::LIMBS / 2;  // u64 words per coordinate
   uint64_t *o = out_proj + (int64_t)i * 3 * H;
+  store_ref<F>(o, X);
+  store_ref<F>(o + H, Y);
+  store_ref<F>(o + 2 * H, Z);
+}
+
+// Horner per MSM of a batch; MSM i writes result slot out_index[i].
+template <class F>
+__global__ void k_combine_indexed(const xyzz_t<F> *__restrict__ S, int n_msm, int W, int c,
+                                  const int32_t *__restrict__ out_index, uint64_t *__restrict__ out_proj) {
+  using FA = typename OutOfLine<F>::type;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_msm) return;
+  xyzz_t<FA> res;
+  xyzz_set_inf(res);
+  for (int w = W - 1; w >= 0; w--) {
+    if (!xyzz_is_inf(res))
+      for (int k = 0; k < c; k++) xyzz_dbl<FA>(res, res);
+    xyzz_add<FA>(res, as_xyzz<FA>(S[(int64_t)i * W + w]));
+  }
+  typename F::T X, Y, Z;
+  xyzz_to_proj<FA>(X, Y, Z, res);
+  constexpr int H = F::LIMBS / 2;
+  uint64_t *o = out_proj + (int64_t)__ldg(out_index + i) * 3 * H;
   store_ref<F>(o, X);
   store_ref<F>(o + H, Y);
   store_ref<F>(o + 2 * H, Z);

@@ -134,6 +134,40 @@ int gm_g2_msm_device_c(gm_stream_t stream, uint32_t gpu_index, G2ProjectivePoint
 int gm_g1_msm_device_noalloc(gm_stream_t stream, uint32_t gpu_index, G1ProjectivePoint *d_result,
                              const G1Point *d_points, const uint64_t *d_scalars, int scalar_limbs, int n);
 
+/* Resident base tables and batched MSMs.  No reference counterpart: every
+ * reference MSM copies and converts its bases again (c_wrapper.cu:64-172).
+ *
+ * gm_bases_create: packs n reference-layout points (device pointer; Montgomery
+ *   form when points_montgomery != 0, else standard form, converted) into an
+ *   owned device table on gpu_index; blocks until done.  n < 2^31.
+ * gm_msm_resident: one MSM over table entries [base_offset, base_offset + n),
+ *   asynchronous on `stream`; result is one projective point of the table's
+ *   group.  window_bits 0 = cost model.
+ * gm_batch_plan_create: fixes a batch of `count` MSMs: MSM i uses table
+ *   entries [base_offsets[i], base_offsets[i] + sizes[i]) (base_offsets may be
+ *   NULL: all 0) and window width window_bits[i] (NULL or 0: cost model).
+ *   MSMs of equal width form a class that runs as one flattened pipeline on
+ *   its own stream.  All workspace is allocated here.
+ * gm_batch_plan_run: enqueues the batch on `stream` (forks the classes and
+ *   joins them back): d_scalars holds the MSMs' scalar rows concatenated in
+ *   MSM order, scalar_limbs u64 each; d_results receives `count` projective
+ *   points in MSM order.  Only kernels, memsets and event waits are enqueued.
+ * gm_batch_plan_classes: window width and MSM count of each class. */
+typedef struct gm_bases gm_bases;
+typedef struct gm_batch_plan gm_batch_plan;
+int gm_bases_create(uint32_t gpu_index, int group, const void *d_points, int64_t n, int points_montgomery,
+                    gm_bases **out);
+int gm_bases_destroy(gm_bases *bases);
+int64_t gm_bases_count(const gm_bases *bases);
+int gm_msm_resident(gm_stream_t stream, const gm_bases *bases, int64_t base_offset, int n, const uint64_t *d_scalars,
+                    int scalar_limbs, void *d_result, int window_bits);
+int gm_batch_plan_create(const gm_bases *bases, int scalar_limbs, int count, const int64_t *sizes,
+                         const int64_t *base_offsets, const int32_t *window_bits, gm_batch_plan **out);
+int gm_batch_plan_run(gm_batch_plan *plan, gm_stream_t stream, const uint64_t *d_scalars, void *d_results);
+int gm_batch_plan_destroy(gm_batch_plan *plan);
+int64_t gm_batch_plan_bytes(const gm_batch_plan *plan);
+int gm_batch_plan_classes(const gm_batch_plan *plan, int32_t *window_bits, int32_t *counts, int max);
+
 /* Window width the cost model picks for an MSM of n points (group 1 or 2). */
 int gm_msm_default_window(int group, int64_t n, int scalar_limbs);
 
