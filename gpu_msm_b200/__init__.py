@@ -61,6 +61,7 @@ C_API = [
     "gm_g1_sum_projective", "gm_g2_sum_projective", "gm_g1_msm_device_noalloc",
     "gm_bases_create", "gm_bases_destroy", "gm_bases_count", "gm_msm_resident", "gm_batch_plan_create",
     "gm_batch_plan_run", "gm_batch_plan_destroy", "gm_batch_plan_bytes", "gm_batch_plan_classes",
+    "gm_batch_run", "gm_batch_workspace_bytes",
 ]
 
 
@@ -101,7 +102,7 @@ def lib() -> ctypes.CDLL:
         L.gm_profile_enable.argtypes = [i32]
         L.gm_profile_collect.argtypes = [ctypes.c_char_p, i32, vp, i32]
         L.gm_launch_count_reset.restype = i64
-        L.gm_imad_probe.argtypes = [vp, u32, i32, vp, i64, vp]
+        L.gm_imad_probe.argtypes = [vp, u32, i32, i32, vp, i64, vp]
         L.gm_g1_msm_device_noalloc.argtypes = [vp, u32, vp, vp, vp, i32, i32]
         L.gm_bases_create.argtypes = [u32, i32, vp, i64, i32, vp]
         L.gm_bases_destroy.argtypes = [vp]
@@ -114,6 +115,9 @@ def lib() -> ctypes.CDLL:
         L.gm_batch_plan_bytes.argtypes = [vp]
         L.gm_batch_plan_bytes.restype = i64
         L.gm_batch_plan_classes.argtypes = [vp, vp, vp, i32]
+        L.gm_batch_run.argtypes = [vp, vp, i32, i32, vp, vp, vp, vp, vp]
+        L.gm_batch_workspace_bytes.argtypes = [vp, i32, i32, vp, vp]
+        L.gm_batch_workspace_bytes.restype = i64
         for name in ("gm_g1_sum_projective", "gm_g2_sum_projective"):
             getattr(L, name).argtypes = [vp, u32, vp, vp, i32]
         _lib = L
@@ -409,13 +413,14 @@ def launch_count_reset() -> int:
     return int(lib().gm_launch_count_reset())
 
 
-def imad_probe(iters: int, sink, stream=None) -> int:
-    """Launch the IMAD throughput probe; returns IMADs per launch."""
+def imad_probe(iters: int, sink, stream=None, mode: int = 0) -> int:
+    """Launch the IMAD throughput probe (mode 0: lo/hi mix, 1: lo only);
+    returns IMADs per launch."""
     import torch
     if not (isinstance(sink, torch.Tensor) and sink.is_cuda and sink.dtype == torch.int32):
         raise ValueError("sink: int32 CUDA tensor")
     cnt = ctypes.c_int64(0)
-    _check(lib().gm_imad_probe(_stream_handle(stream), _dev_index(sink), iters, ctypes.c_void_p(sink.data_ptr()),
+    _check(lib().gm_imad_probe(_stream_handle(stream), _dev_index(sink), iters, mode, ctypes.c_void_p(sink.data_ptr()),
                                sink.numel(), ctypes.byref(cnt)), "imad_probe")
     return cnt.value
 
@@ -549,3 +554,35 @@ class BatchPlan:
             self.close()
         except Exception:
             pass
+
+
+def batch_run(bases: ResidentBases, sizes, scalars, base_offsets=None, window_bits=None, out=None, stream=None):
+    """One batch without a plan (``gm_batch_run``): workspace from the stream-
+    ordered pool, classes in order on the stream.  For batches whose shape
+    changes on every call."""
+    import torch
+    sizes = np.ascontiguousarray(sizes, dtype=np.int64)
+    total = int(sizes.sum())
+    _require(scalars, None, "scalars", rows=total)
+    if window_bits is None:
+        window_bits = [tuned_window(bases.group, int(s), scalars.shape[1]) for s in sizes]
+    wins = np.ascontiguousarray(window_bits, dtype=np.int32)
+    offs = None if base_offsets is None else np.ascontiguousarray(base_offsets, dtype=np.int64)
+    words = G1P_WORDS if bases.group == 1 else G2P_WORDS
+    if out is None:
+        out = torch.empty((len(sizes), words), dtype=torch.int64, device=scalars.device)
+    _check(lib().gm_batch_run(_stream_handle(stream), bases.handle, scalars.shape[1], len(sizes), _p(sizes),
+                              None if offs is None else _p(offs), _p(wins), ctypes.c_void_p(scalars.data_ptr()),
+                              ctypes.c_void_p(out.data_ptr())), "gm_batch_run")
+    return out
+
+
+def batch_workspace_bytes(bases: ResidentBases, sizes, window_bits=None, scalar_limbs: int = 5) -> int:
+    sizes = np.ascontiguousarray(sizes, dtype=np.int64)
+    if window_bits is None:
+        window_bits = [tuned_window(bases.group, int(s), scalar_limbs) for s in sizes]
+    wins = np.ascontiguousarray(window_bits, dtype=np.int32)
+    v = int(lib().gm_batch_workspace_bytes(bases.handle, scalar_limbs, len(sizes), _p(sizes), _p(wins)))
+    if v < 0:
+        raise MSMError("gm_batch_workspace_bytes: bad batch")
+    return v

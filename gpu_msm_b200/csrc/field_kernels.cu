@@ -64,20 +64,28 @@ int launch_field(gm_stream_t stream, uint32_t gpu_index, void *c, const void *a,
   return e == cudaSuccess ? gm::GM_OK : gm::record_error(e, "k_field_mul");
 }
 
-// IMAD-pipe throughput probe: 16 independent accumulator chains per thread,
-// each iteration issuing 8 mad.lo.u32 and 8 mad.hi.u32 (16 IMAD) whose only
-// dependency is on the same chain's previous value.  Used to measure the
-// integer multiply-add peak that the MSM roofline is quoted against.
-__global__ void __launch_bounds__(256) k_imad_probe(uint32_t *__restrict__ sink, int iters, uint32_t seed) {
+// IMAD-pipe throughput probe: 16 independent accumulator chains per thread.
+// mode 0 issues 8 mad.lo.u32 + 8 mad.hi.u32 per iteration (the lo/hi mix of a
+// Montgomery product), mode 1 issues 16 mad.lo.u32.  Each chain depends only
+// on its own previous value.  Used to measure the integer multiply-add
+// ceiling that the MSM roofline is quoted against.
+__global__ void __launch_bounds__(256) k_imad_probe(uint32_t *__restrict__ sink, int iters, uint32_t seed, int mode) {
   uint32_t a[16];
 #pragma unroll
   for (int k = 0; k < 16; k++) a[k] = seed * (threadIdx.x + 1) + 0x9e3779b9u * (k + 1);
   const uint32_t m = seed | 1u, c = seed ^ 0x85ebca6bu;
-  for (int it = 0; it < iters; it++) {
+  if (mode == 0) {
+    for (int it = 0; it < iters; it++) {
 #pragma unroll
-    for (int k = 0; k < 16; k += 2) {
-      asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(a[k]) : "r"(m), "r"(c));
-      asm volatile("mad.hi.u32 %0, %0, %1, %2;" : "+r"(a[k + 1]) : "r"(m), "r"(c));
+      for (int k = 0; k < 16; k += 2) {
+        asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(a[k]) : "r"(m), "r"(c));
+        asm volatile("mad.hi.u32 %0, %0, %1, %2;" : "+r"(a[k + 1]) : "r"(m), "r"(c));
+      }
+    }
+  } else {
+    for (int it = 0; it < iters; it++) {
+#pragma unroll
+      for (int k = 0; k < 16; k++) asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(a[k]) : "r"(m), "r"(c));
     }
   }
   uint32_t x = 0;
@@ -90,15 +98,15 @@ __global__ void __launch_bounds__(256) k_imad_probe(uint32_t *__restrict__ sink,
 
 extern "C" {
 
-int gm_imad_probe(gm_stream_t stream, uint32_t gpu_index, int iters, uint32_t *d_sink, int64_t sink_words,
-                  int64_t *imad_per_launch) {
+int gm_imad_probe(gm_stream_t stream, uint32_t gpu_index, int iters, int mode, uint32_t *d_sink,
+                  int64_t sink_words, int64_t *imad_per_launch) {
   int rc = gm::select_device(gpu_index);
   if (rc) return rc;
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_imad_probe, 256, 0);
   const int64_t blocks = (int64_t)sm_count((int)gpu_index) * (per_sm > 0 ? per_sm : 1);
   if (blocks * 256 > sink_words || iters <= 0) return gm::GM_ERR_ARG;
-  k_imad_probe<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(d_sink, iters, 0x2545f491u);
+  k_imad_probe<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(d_sink, iters, 0x2545f491u, mode);
   gm::count_launches(1);
   if (imad_per_launch) *imad_per_launch = blocks * 256 * (int64_t)iters * 16;
   cudaError_t e = cudaGetLastError();

@@ -48,6 +48,80 @@ void free_plan(gm_batch_plan *p) {
   delete p;
 }
 
+// Validates the batch, groups MSMs by window width and computes each class's
+// layout; d64[k] / idx[k] receive class k's descriptors
+// (point_start | base_off | sc_off, and out_index).
+int build_classes(const gm_bases *b, int scalar_limbs, int count, const int64_t *sizes, const int64_t *base_offsets,
+                  const int32_t *window_bits, gm::BatchPlan &plan, std::vector<std::vector<int64_t>> &d64,
+                  std::vector<std::vector<int32_t>> &idx) {
+  if (!b || count <= 0 || !sizes || scalar_limbs < 1 || scalar_limbs > gm::MAX_SCALAR_LIMBS) return gm::GM_ERR_ARG;
+  int rc = gm::select_device((uint32_t)b->dev);
+  if (rc) return rc;
+  std::map<int, std::vector<int>> by_c;
+  std::vector<int64_t> sc_row(count + 1, 0);
+  for (int i = 0; i < count; i++) {
+    const int64_t off = base_offsets ? base_offsets[i] : 0;
+    if (sizes[i] <= 0 || off < 0 || off + sizes[i] > b->n) {
+      gm::set_last_error("batch MSM outside the base table or empty");
+      return gm::GM_ERR_ARG;
+    }
+    sc_row[i + 1] = sc_row[i] + sizes[i];
+    const int c =
+        window_bits && window_bits[i] > 0 ? window_bits[i] : gm::default_window(b->group, sizes[i], scalar_limbs);
+    if (c < 2 || c > 20) {
+      gm::set_last_error("window width out of range");
+      return gm::GM_ERR_ARG;
+    }
+    by_c[c].push_back(i);
+  }
+  plan.group = b->group;
+  plan.dev = b->dev;
+  plan.limbs = scalar_limbs;
+  plan.count = count;
+  plan.bases = b->packed;
+  plan.n_bases = b->n;
+  plan.classes.clear();
+  for (auto &kv : by_c) {
+    gm::BatchClassPlan cp;
+    cp.c = kv.first;
+    cp.count = (int)kv.second.size();
+    for (int i : kv.second) cp.P += sizes[i];
+    plan.classes.push_back(cp);
+  }
+  int sms = 0;
+  rc = gm::device_sm_count(b->dev, &sms);
+  if (rc) return rc;
+  if (b->group == 1)
+    gm::batch_layouts<gm::Fp>(plan, sms);
+  else
+    gm::batch_layouts<gm::Fp2>(plan, sms);
+  d64.assign(plan.classes.size(), {});
+  idx.assign(plan.classes.size(), {});
+  size_t k = 0;
+  for (auto &kv : by_c) {
+    gm::BatchClassPlan &cp = plan.classes[k];
+    if ((uint64_t)cp.P * cp.dp.W >= (1ull << 32)) {
+      gm::set_last_error("batch class too large for 32-bit entry offsets");
+      return gm::GM_ERR_ARG;
+    }
+    std::vector<int64_t> &v = d64[k];
+    v.assign(3 * (size_t)cp.count + 1, 0);
+    idx[k].assign(cp.count, 0);
+    int64_t acc = 0;
+    for (int j = 0; j < cp.count; j++) {
+      const int i = kv.second[j];
+      v[j] = acc;
+      acc += sizes[i];
+      v[cp.count + 1 + j] = base_offsets ? base_offsets[i] : 0;
+      v[2 * cp.count + 1 + j] = sc_row[i];
+      idx[k][j] = i;
+    }
+    v[cp.count] = acc;
+    k++;
+  }
+  return gm::GM_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -114,81 +188,24 @@ int gm_msm_resident(gm_stream_t stream, const gm_bases *b, int64_t base_offset, 
 
 int gm_batch_plan_create(const gm_bases *b, int scalar_limbs, int count, const int64_t *sizes,
                          const int64_t *base_offsets, const int32_t *window_bits, gm_batch_plan **out) {
-  if (!b || !out || count <= 0 || !sizes || scalar_limbs < 1 || scalar_limbs > gm::MAX_SCALAR_LIMBS)
-    return gm::GM_ERR_ARG;
-  int rc = gm::select_device((uint32_t)b->dev);
-  if (rc) return rc;
-  // validate and group MSMs by window width
-  std::map<int, std::vector<int>> by_c;
-  std::vector<int64_t> sc_row(count + 1, 0);
-  for (int i = 0; i < count; i++) {
-    const int64_t off = base_offsets ? base_offsets[i] : 0;
-    if (sizes[i] <= 0 || off < 0 || off + sizes[i] > b->n) {
-      gm::set_last_error("batch MSM outside the base table or empty");
-      return gm::GM_ERR_ARG;
-    }
-    sc_row[i + 1] = sc_row[i] + sizes[i];
-    int c = window_bits && window_bits[i] > 0 ? window_bits[i] : gm::default_window(b->group, sizes[i], scalar_limbs);
-    if (c < 2 || c > 20) {
-      gm::set_last_error("window width out of range");
-      return gm::GM_ERR_ARG;
-    }
-    by_c[c].push_back(i);
-  }
+  if (!b || !out) return gm::GM_ERR_ARG;
   auto *p = new (std::nothrow) gm_batch_plan;
   if (!p) return gm::GM_ERR_ALLOC;
-  gm::BatchPlan &plan = p->plan;
-  plan.group = b->group;
-  plan.dev = b->dev;
-  plan.limbs = scalar_limbs;
-  plan.count = count;
-  plan.bases = b->packed;
-  plan.n_bases = b->n;
-  for (auto &kv : by_c) {
-    gm::BatchClassPlan cp;
-    cp.c = kv.first;
-    cp.count = (int)kv.second.size();
-    int64_t P = 0;
-    for (int i : kv.second) P += sizes[i];
-    cp.P = P;
-    plan.classes.push_back(cp);
-  }
-  int sms = 0;
-  rc = gm::device_sm_count(b->dev, &sms);
+  std::vector<std::vector<int64_t>> d64;
+  std::vector<std::vector<int32_t>> idx;
+  int rc = build_classes(b, scalar_limbs, count, sizes, base_offsets, window_bits, p->plan, d64, idx);
   if (rc) {
-    free_plan(p);
+    delete p;
     return rc;
   }
-  if (b->group == 1)
-    gm::batch_layouts<gm::Fp>(plan, sms);
-  else
-    gm::batch_layouts<gm::Fp2>(plan, sms);
-  size_t ci = 0;
-  for (auto &kv : by_c) {
-    gm::BatchClassPlan &cp = plan.classes[ci++];
-    if ((uint64_t)cp.P * cp.dp.W >= (1ull << 32)) {
-      free_plan(p);
-      gm::set_last_error("batch class too large for 32-bit entry offsets");
-      return gm::GM_ERR_ARG;
-    }
-    // descriptors: point_start[count+1] | base_off[count] | sc_off[count] | out_index[count] (int32)
-    std::vector<int64_t> d64(3 * (size_t)cp.count + 1);
-    std::vector<int32_t> idx(cp.count);
-    int64_t acc = 0;
-    for (int k = 0; k < cp.count; k++) {
-      const int i = kv.second[k];
-      d64[k] = acc;
-      acc += sizes[i];
-      d64[cp.count + 1 + k] = base_offsets ? base_offsets[i] : 0;
-      d64[2 * cp.count + 1 + k] = sc_row[i];
-      idx[k] = i;
-    }
-    d64[cp.count] = acc;
-    const size_t desc_bytes = d64.size() * sizeof(int64_t) + idx.size() * sizeof(int32_t);
+  gm::BatchPlan &plan = p->plan;
+  for (size_t k = 0; k < plan.classes.size(); k++) {
+    gm::BatchClassPlan &cp = plan.classes[k];
+    const size_t desc_bytes = d64[k].size() * sizeof(int64_t) + idx[k].size() * sizeof(int32_t);
     cudaError_t e = cudaMalloc(&cp.desc, desc_bytes);
-    if (e == cudaSuccess) e = cudaMemcpy(cp.desc, d64.data(), d64.size() * sizeof(int64_t), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(cp.desc, d64[k].data(), d64[k].size() * sizeof(int64_t), cudaMemcpyHostToDevice);
     if (e == cudaSuccess)
-      e = cudaMemcpy(cp.desc + d64.size() * sizeof(int64_t), idx.data(), idx.size() * sizeof(int32_t),
+      e = cudaMemcpy(cp.desc + d64[k].size() * sizeof(int64_t), idx[k].data(), idx[k].size() * sizeof(int32_t),
                      cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMalloc(&cp.ws, cp.ws_bytes);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&cp.stream, cudaStreamNonBlocking);
@@ -207,6 +224,77 @@ int gm_batch_plan_create(const gm_bases *b, int scalar_limbs, int count, const i
   }
   *out = p;
   return gm::GM_OK;
+}
+
+int64_t gm_batch_workspace_bytes(const gm_bases *b, int scalar_limbs, int count, const int64_t *sizes,
+                                 const int32_t *window_bits) {
+  gm::BatchPlan plan;
+  std::vector<std::vector<int64_t>> d64;
+  std::vector<std::vector<int32_t>> idx;
+  if (build_classes(b, scalar_limbs, count, sizes, nullptr, window_bits, plan, d64, idx)) return -1;
+  int64_t bytes = 0;
+  for (size_t k = 0; k < plan.classes.size(); k++)
+    bytes += (int64_t)(plan.classes[k].ws_bytes + d64[k].size() * sizeof(int64_t) + idx[k].size() * sizeof(int32_t) +
+                       512);
+  return bytes;
+}
+
+int gm_batch_run(gm_stream_t stream, const gm_bases *b, int scalar_limbs, int count, const int64_t *sizes,
+                 const int64_t *base_offsets, const int32_t *window_bits, const uint64_t *d_scalars,
+                 void *d_results) {
+  if (!d_scalars || !d_results) return gm::GM_ERR_ARG;
+  gm::BatchPlan plan;
+  std::vector<std::vector<int64_t>> d64;
+  std::vector<std::vector<int32_t>> idx;
+  int rc = build_classes(b, scalar_limbs, count, sizes, base_offsets, window_bits, plan, d64, idx);
+  if (rc) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  // one stream-ordered allocation: every class's descriptors first (so they
+  // can be staged contiguously), then the workspaces
+  std::vector<size_t> off_desc(plan.classes.size()), off_ws(plan.classes.size());
+  size_t total = 0;
+  for (size_t k = 0; k < plan.classes.size(); k++) {
+    off_desc[k] = total;
+    total += (d64[k].size() * sizeof(int64_t) + idx[k].size() * sizeof(int32_t) + 255) / 256 * 256;
+  }
+  const size_t desc_total = total;
+  for (size_t k = 0; k < plan.classes.size(); k++) {
+    off_ws[k] = total;
+    total += (plan.classes[k].ws_bytes + 255) / 256 * 256;
+  }
+  char *mem = nullptr;
+  rc = gm::pool_alloc(plan.dev, s, total, (void **)&mem);
+  if (rc) return rc;
+  // descriptors go through one pinned slot (an asynchronous copy from pageable
+  // memory would first wait for the stream), released in stream order
+  void *slot = nullptr;
+  const bool pinned = desc_total <= gm::PINNED_SLOT_BYTES && gm::pinned_acquire(&slot) == gm::GM_OK;
+  for (size_t k = 0; k < plan.classes.size(); k++) {
+    gm::BatchClassPlan &cp = plan.classes[k];
+    cp.desc = mem + off_desc[k];
+    cp.ws = mem + off_ws[k];
+    const size_t n64 = d64[k].size() * sizeof(int64_t), n32 = idx[k].size() * sizeof(int32_t);
+    cudaError_t e;
+    if (pinned) {
+      char *h = static_cast<char *>(slot) + off_desc[k];
+      memcpy(h, d64[k].data(), n64);
+      memcpy(h + n64, idx[k].data(), n32);
+      e = cudaMemcpyAsync(cp.desc, h, n64 + n32, cudaMemcpyHostToDevice, s);
+    } else {
+      e = cudaMemcpyAsync(cp.desc, d64[k].data(), n64, cudaMemcpyHostToDevice, s);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(cp.desc + n64, idx[k].data(), n32, cudaMemcpyHostToDevice, s);
+    }
+    if (e != cudaSuccess) {
+      if (pinned) gm::enqueue_pinned_release(s, slot);
+      cudaFreeAsync(mem, s);
+      return gm::record_error(e, "batch descriptors");
+    }
+  }
+  if (pinned) gm::enqueue_pinned_release(s, slot);
+  rc = plan.group == 1 ? gm::batch_run<gm::Fp>(plan, s, d_scalars, (uint64_t *)d_results)
+                       : gm::batch_run<gm::Fp2>(plan, s, d_scalars, (uint64_t *)d_results);
+  cudaFreeAsync(mem, s);
+  return rc;
 }
 
 int gm_batch_plan_run(gm_batch_plan *p, gm_stream_t stream, const uint64_t *d_scalars, void *d_results) {

@@ -147,10 +147,18 @@ int batch_layouts(BatchPlan &plan, int sms) {
   return GM_OK;
 }
 
-// Fork the classes onto their streams and join them back into `s`.
+// Fork the classes onto their streams and join them back into `s` (plans
+// with their own streams), or run them in order on `s`.
 template <class F>
 int batch_run(const BatchPlan &plan, cudaStream_t s, const uint64_t *scalars, uint64_t *results) {
-  if (plan.classes.size() == 1) return batch_class_run<F>(plan, plan.classes[0], s, scalars, results);
+  if (plan.classes.size() == 1 || plan.fork == nullptr) {
+    // one class, or a transient plan without its own streams: in order on s
+    for (const auto &cp : plan.classes) {
+      const int rc = batch_class_run<F>(plan, cp, s, scalars, results);
+      if (rc) return rc;
+    }
+    return GM_OK;
+  }
   GM_CHECK(cudaEventRecord(plan.fork, s));
   for (const auto &cp : plan.classes) {
     GM_CHECK(cudaStreamWaitEvent(cp.stream, plan.fork, 0));

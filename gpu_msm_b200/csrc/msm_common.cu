@@ -149,7 +149,7 @@ int64_t launches_and_reset() {
 // ---------------------------------------------------------------------------
 // host tail: pinned slots and stream-ordered host functions
 // ---------------------------------------------------------------------------
-static constexpr size_t TAIL_SLOT_BYTES = 128 * 1024;  // >= 257 windows x 448 B + 336 B
+constexpr size_t TAIL_SLOT_BYTES = PINNED_SLOT_BYTES;  // >= 257 windows x 448 B + 336 B
 static std::mutex g_pin_mu;
 static std::vector<void *> g_pin_free;
 static bool g_host_tail = true;
@@ -157,7 +157,7 @@ static bool g_host_tail = true;
 bool host_tail_enabled() { return g_host_tail; }
 void set_host_tail_enabled(bool on) { g_host_tail = on; }
 
-static int pinned_acquire(void **p) {
+int pinned_acquire(void **p) {
   {
     std::lock_guard<std::mutex> lk(g_pin_mu);
     if (!g_pin_free.empty()) {
@@ -166,12 +166,12 @@ static int pinned_acquire(void **p) {
       return GM_OK;
     }
   }
-  cudaError_t e = cudaMallocHost(p, TAIL_SLOT_BYTES);
+  cudaError_t e = cudaMallocHost(p, PINNED_SLOT_BYTES);
   if (e != cudaSuccess) return record_error(e, "cudaMallocHost(tail slot)");
   return GM_OK;
 }
 
-static void pinned_release(void *p) {
+void pinned_release(void *p) {
   std::lock_guard<std::mutex> lk(g_pin_mu);
   g_pin_free.push_back(p);
 }
@@ -192,6 +192,13 @@ static void CUDART_CB tail_compute(void *p) {
     gm_host::horner_to_proj<gm_host::F2>(out, reinterpret_cast<const gm_host::HXyzz<gm_host::F2> *>(t->slot), t->W,
                                          t->c);
   }
+}
+
+static void CUDART_CB slot_release(void *p) { pinned_release(p); }
+
+int enqueue_pinned_release(cudaStream_t s, void *slot) {
+  cudaError_t e = cudaLaunchHostFunc(s, slot_release, slot);
+  return e == cudaSuccess ? GM_OK : record_error(e, "cudaLaunchHostFunc(release)");
 }
 
 static void CUDART_CB tail_release(void *p) {

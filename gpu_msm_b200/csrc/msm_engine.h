@@ -36,6 +36,12 @@ int profile_collect(char *names, int names_len, float *ms, int max);
 // stream is being captured.
 int enqueue_host_tail(cudaStream_t s, int group, const void *d_sums, int W, int c, uint64_t *d_out);
 bool host_tail_enabled();
+// Pinned host slots of PINNED_SLOT_BYTES, recycled; enqueue_pinned_release
+// hands a slot back once the stream reaches that point.
+constexpr size_t PINNED_SLOT_BYTES = 128 * 1024;
+int pinned_acquire(void **p);
+void pinned_release(void *p);
+int enqueue_pinned_release(cudaStream_t s, void *slot);
 void set_host_tail_enabled(bool on);
 // kernel launches issued by this host thread since the last reset
 void count_launches(int k);

@@ -152,7 +152,13 @@ int gm_g1_msm_device_noalloc(gm_stream_t stream, uint32_t gpu_index, G1Projectiv
  *   joins them back): d_scalars holds the MSMs' scalar rows concatenated in
  *   MSM order, scalar_limbs u64 each; d_results receives `count` projective
  *   points in MSM order.  Only kernels, memsets and event waits are enqueued.
- * gm_batch_plan_classes: window width and MSM count of each class. */
+ * gm_batch_plan_classes: window width and MSM count of each class.
+ * gm_batch_run: the same batch without a plan: workspace and descriptors come
+ *   from the per-device stream-ordered pool for this one run and the classes
+ *   run in order on `stream` (for batches whose shape changes every time, as
+ *   in serving).
+ * gm_batch_workspace_bytes: device bytes gm_batch_run takes for that batch
+ *   (for admission control), or -1 on a bad argument. */
 typedef struct gm_bases gm_bases;
 typedef struct gm_batch_plan gm_batch_plan;
 int gm_bases_create(uint32_t gpu_index, int group, const void *d_points, int64_t n, int points_montgomery,
@@ -167,6 +173,10 @@ int gm_batch_plan_run(gm_batch_plan *plan, gm_stream_t stream, const uint64_t *d
 int gm_batch_plan_destroy(gm_batch_plan *plan);
 int64_t gm_batch_plan_bytes(const gm_batch_plan *plan);
 int gm_batch_plan_classes(const gm_batch_plan *plan, int32_t *window_bits, int32_t *counts, int max);
+int gm_batch_run(gm_stream_t stream, const gm_bases *bases, int scalar_limbs, int count, const int64_t *sizes,
+                 const int64_t *base_offsets, const int32_t *window_bits, const uint64_t *d_scalars, void *d_results);
+int64_t gm_batch_workspace_bytes(const gm_bases *bases, int scalar_limbs, int count, const int64_t *sizes,
+                                 const int32_t *window_bits);
 
 /* Window width the cost model picks for an MSM of n points (group 1 or 2). */
 int gm_msm_default_window(int group, int64_t n, int scalar_limbs);
@@ -217,13 +227,14 @@ int gm_g2_sum_projective(gm_stream_t stream, uint32_t gpu_index, G2ProjectivePoi
  * gm_launch_count_reset: number of kernels this library launched from the
  *   calling thread since the previous call.
  * gm_imad_probe: launches a kernel of independent 32-bit IMAD chains over
- *   the whole GPU; *imad_per_launch receives the IMAD count so that the caller
- *   can time it and derive the integer multiply-add peak. */
+ *   the whole GPU (mode 0: half mad.lo, half mad.hi, the mix of a Montgomery
+ *   product; mode 1: mad.lo only); *imad_per_launch receives the IMAD count
+ *   so that the caller can time it and derive the multiply-add ceiling. */
 int gm_profile_enable(int on);
 int gm_profile_collect(char *names, int names_len, float *ms, int max);
 int64_t gm_launch_count_reset(void);
-int gm_imad_probe(gm_stream_t stream, uint32_t gpu_index, int iters, uint32_t *d_sink, int64_t sink_words,
-                  int64_t *imad_per_launch);
+int gm_imad_probe(gm_stream_t stream, uint32_t gpu_index, int iters, int mode, uint32_t *d_sink,
+                  int64_t sink_words, int64_t *imad_per_launch);
 
 /* Last CUDA error string seen by this library on the calling thread. */
 const char *gm_last_error(void);
