@@ -61,7 +61,7 @@ C_API = [
     "gm_g1_sum_projective", "gm_g2_sum_projective", "gm_g1_msm_device_noalloc",
     "gm_bases_create", "gm_bases_destroy", "gm_bases_count", "gm_msm_resident", "gm_batch_plan_create",
     "gm_batch_plan_run", "gm_batch_plan_destroy", "gm_batch_plan_bytes", "gm_batch_plan_classes",
-    "gm_batch_run", "gm_batch_workspace_bytes",
+    "gm_batch_run", "gm_batch_workspace_bytes", "gm_g1_sum_projective_host",
 ]
 
 
@@ -116,6 +116,7 @@ def lib() -> ctypes.CDLL:
         L.gm_batch_plan_bytes.restype = i64
         L.gm_batch_plan_classes.argtypes = [vp, vp, vp, i32]
         L.gm_batch_run.argtypes = [vp, vp, i32, i32, vp, vp, vp, vp, vp]
+        L.gm_g1_sum_projective_host.argtypes = [vp, vp, i32]
         L.gm_batch_workspace_bytes.argtypes = [vp, i32, i32, vp, vp]
         L.gm_batch_workspace_bytes.restype = i64
         for name in ("gm_g1_sum_projective", "gm_g2_sum_projective"):
@@ -335,6 +336,14 @@ def sum_projective(points, group: int = 1, out=None, stream=None):
     fn = lib().gm_g1_sum_projective if group == 1 else lib().gm_g2_sum_projective
     _check(fn(_stream_handle(stream), _dev_index(points), ctypes.c_void_p(out.data_ptr()),
               ctypes.c_void_p(points.data_ptr()), points.shape[0]), "sum_projective")
+    return out
+
+
+def sum_projective_host(points: np.ndarray) -> np.ndarray:
+    """Host-side sum of G1 projective points (numpy G1P array)."""
+    pts = np.ascontiguousarray(points, dtype=G1P).reshape(-1)
+    out = np.zeros(1, dtype=G1P)
+    _check(lib().gm_g1_sum_projective_host(_p(out), _p(pts), len(pts)), "gm_g1_sum_projective_host")
     return out
 
 

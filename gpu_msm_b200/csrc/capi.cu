@@ -521,6 +521,32 @@ int gm_g2_sum_projective(gm_stream_t stream, uint32_t gpu_index, G2ProjectivePoi
   return e == cudaSuccess ? gm::GM_OK : gm::record_error(e, "k_proj_sum");
 }
 
+int gm_g1_sum_projective_host(G1ProjectivePoint *out, const G1ProjectivePoint *in, int n) {
+  if (n < 0 || out == nullptr || (n > 0 && in == nullptr)) return gm::GM_ERR_ARG;
+  gm_host::HXyzz<gm_host::F1> acc;
+  memset(&acc, 0, sizeof(acc));
+  for (int i = 0; i < n; i++) {
+    // homogeneous (X, Y, Z) -> XYZZ (X Z, Y Z^2, Z^2, Z^3)
+    gm_host::HXyzz<gm_host::F1> p;
+    memset(&p, 0, sizeof(p));
+    if (!gm_host::is_zero(in[i].Z.limb)) {
+      gm_host::F1::T X, Y, Z;
+      memcpy(X.v, in[i].X.limb, 56);
+      memcpy(Y.v, in[i].Y.limb, 56);
+      memcpy(Z.v, in[i].Z.limb, 56);
+      gm_host::F1::mul(p.ZZ, Z, Z);
+      gm_host::F1::mul(p.ZZZ, p.ZZ, Z);
+      gm_host::F1::mul(p.X, X, Z);
+      gm_host::F1::mul(p.Y, Y, p.ZZ);
+    }
+    gm_host::hx_add(acc, p);
+  }
+  uint64_t words[21];
+  gm_host::horner_to_proj<gm_host::F1>(words, &acc, 1, 0);
+  memcpy(out, words, sizeof(words));
+  return gm::GM_OK;
+}
+
 const char *gm_last_error(void) { return gm::last_error(); }
 
 }  // extern "C"

@@ -218,6 +218,10 @@ int gm_g1_sum_projective(gm_stream_t stream, uint32_t gpu_index, G1ProjectivePoi
 int gm_g2_sum_projective(gm_stream_t stream, uint32_t gpu_index, G2ProjectivePoint *d_out,
                          const G2ProjectivePoint *d_in, int n);
 
+/* Host-side sum of n G1 projective points (Montgomery form): combines the
+ * partial results of a sharded MSM on a CPU; no reference counterpart. */
+int gm_g1_sum_projective_host(G1ProjectivePoint *out, const G1ProjectivePoint *in, int n);
+
 /* Measurement hooks (no reference counterpart).
  * gm_profile_enable: while on, every MSM records CUDA events on its stream at
  *   its phase boundaries (pack, sort, accumulate, fixup, reduce, combine).
