@@ -55,6 +55,7 @@ C_API = [
     "g1_msm_limbs_wrapper", "g2_msm_limbs_wrapper", "gm_g1_msm_device", "gm_g2_msm_device",
     "gm_g1_msm_device_c", "gm_g2_msm_device_c", "gm_msm_default_window",
     "gm_fp_mont_mul_array", "gm_fp_mul_array", "gm_fp2_mont_mul_array", "gm_fp2_mul_array",
+    "gm_fp_mont_sqr_array",
     "gm_g1_to_montgomery_batch", "gm_g2_to_montgomery_batch",
     "gm_g1_generator_mul_batch", "gm_g2_generator_mul_batch", "gm_last_error",
     "gm_profile_enable", "gm_profile_collect", "gm_launch_count_reset", "gm_imad_probe",
@@ -91,6 +92,7 @@ def lib() -> ctypes.CDLL:
         L.gm_msm_default_window.argtypes = [i32, i64, i32]
         for name in ("gm_fp_mont_mul_array", "gm_fp_mul_array", "gm_fp2_mont_mul_array", "gm_fp2_mul_array"):
             getattr(L, name).argtypes = [vp, u32, vp, vp, vp, i64]
+        L.gm_fp_mont_sqr_array.argtypes = [vp, u32, vp, vp, i64]
         for name in ("gm_g1_to_montgomery_batch", "gm_g2_to_montgomery_batch"):
             getattr(L, name).argtypes = [vp, u32, vp, i32]
         for name in ("gm_g1_generator_mul_batch", "gm_g2_generator_mul_batch"):
@@ -384,6 +386,19 @@ def field_mul_array(a, b, op: str = "fp_mont_mul", out=None, stream=None):
     fn = getattr(lib(), f"gm_{op}_array")
     _check(fn(_stream_handle(stream), _dev_index(a), ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(a.data_ptr()),
               ctypes.c_void_p(b.data_ptr()), a.shape[0]), op)
+    return out
+
+
+def field_sqr_array(a, out=None, stream=None):
+    """Element-wise Montgomery squares a^2 R^-1 of an (n, 7) int64 device
+    tensor of Fp elements (the dedicated squaring of the point formulas)."""
+    import torch
+    _require(a, 7, "a")
+    if out is None:
+        out = torch.empty_like(a)
+    _require(out, 7, "out", rows=a.shape[0])
+    _check(lib().gm_fp_mont_sqr_array(_stream_handle(stream), _dev_index(a), ctypes.c_void_p(out.data_ptr()),
+                                      ctypes.c_void_p(a.data_ptr()), a.shape[0]), "fp_mont_sqr")
     return out
 
 

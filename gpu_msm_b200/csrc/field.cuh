@@ -270,6 +270,123 @@ GM_DEVI void mont_mul_raw(uint32_t r[NL], const uint32_t a[NL], const uint32_t b
 }
 
 // ---------------------------------------------------------------------------
+// Montgomery squaring (separated operand scanning): the 91 cross products
+// a_i*a_j (i < j) are formed once, doubled by a one-bit shift, and the 14
+// squares a_i^2 are added on the diagonal; the 28-word square is then reduced
+// by the same 14 quotient rows as mont_mul_raw.  301 products instead of 392;
+// measured 1.25x the throughput of mont_mul_raw(a, a) on B200 with identical
+// (canonical) results.
+//
+// Cross products of row i go to two accumulators by the parity of j - i - 1
+// (A: words 2i+1.., B: words 2i+2..), so each chain's words are disjoint and
+// one carry flag suffices per chain.  A chain's carry-out word was last
+// written as a previous chain's carry-out (value <= 1) or is still zero, so
+// adding the carry never overflows.
+// ---------------------------------------------------------------------------
+template <bool STRICT>
+GM_DEVI void mont_sqr_raw(uint32_t r[NL], const uint32_t a[NL]) {
+  uint32_t A[2 * NL], B[2 * NL];
+#pragma unroll
+  for (int k = 0; k < 2 * NL; k++) {
+    A[k] = 0;
+    B[k] = 0;
+  }
+#pragma unroll
+  for (int i = 0; i < NL - 1; i++) {
+    {
+      int j = i + 1;
+      A[i + j] = mad_lo_cc(a[i], a[j], A[i + j]);
+      A[i + j + 1] = madc_hi_cc(a[i], a[j], A[i + j + 1]);
+      int top = i + j + 1;
+#pragma unroll
+      for (j = i + 3; j < NL; j += 2) {
+        A[i + j] = madc_lo_cc(a[i], a[j], A[i + j]);
+        A[i + j + 1] = madc_hi_cc(a[i], a[j], A[i + j + 1]);
+        top = i + j + 1;
+      }
+      if (top + 1 < 2 * NL) A[top + 1] = addc(A[top + 1], 0);
+    }
+    if (i + 2 < NL) {
+      int j = i + 2;
+      B[i + j] = mad_lo_cc(a[i], a[j], B[i + j]);
+      B[i + j + 1] = madc_hi_cc(a[i], a[j], B[i + j + 1]);
+      int top = i + j + 1;
+#pragma unroll
+      for (j = i + 4; j < NL; j += 2) {
+        B[i + j] = madc_lo_cc(a[i], a[j], B[i + j]);
+        B[i + j + 1] = madc_hi_cc(a[i], a[j], B[i + j + 1]);
+        top = i + j + 1;
+      }
+      if (top + 1 < 2 * NL) B[top + 1] = addc(B[top + 1], 0);
+    }
+  }
+  // T = 2 (A + B) + diagonal; the cross sum is below 2^(2*448-1)
+  uint32_t T[2 * NL];
+  T[0] = add_cc(A[0], B[0]);
+#pragma unroll
+  for (int k = 1; k < 2 * NL; k++) T[k] = addc_cc(A[k], B[k]);
+#pragma unroll
+  for (int k = 2 * NL - 1; k > 0; k--) T[k] = __funnelshift_l(T[k - 1], T[k], 1);
+  T[0] <<= 1;
+  T[0] = mad_lo_cc(a[0], a[0], T[0]);
+  T[1] = madc_hi_cc(a[0], a[0], T[1]);
+#pragma unroll
+  for (int i = 1; i < NL; i++) {
+    T[2 * i] = madc_lo_cc(a[i], a[i], T[2 * i]);
+    T[2 * i + 1] = madc_hi_cc(a[i], a[i], T[2 * i + 1]);
+  }
+  // reduction: X = low half of T plus the even quotient products, Y the odd
+  // ones (one word up); the high half of T is added at the end
+  uint32_t X[2 * NL], Y[2 * NL];
+#pragma unroll
+  for (int k = 0; k < NL; k++) {
+    X[k] = T[k];
+    Y[k] = 0;
+  }
+  uint32_t c = 0;
+#pragma unroll
+  for (int i = 0; i < NL; i++) {
+    const uint32_t u = (i == 0) ? X[0] : X[i] + Y[i - 1] + c;
+    const uint32_t m = u * FpConst::PINV;
+    X[i] = mad_lo_cc(m, FpConst::P(0), X[i]);
+    X[i + 1] = madc_hi_cc(m, FpConst::P(0), X[i + 1]);
+#pragma unroll
+    for (int j = 2; j < NL; j += 2) {
+      X[i + j] = madc_lo_cc(m, FpConst::P(j), X[i + j]);
+      X[i + j + 1] = madc_hi_cc(m, FpConst::P(j), X[i + j + 1]);
+    }
+    X[i + NL] = addc(0, 0);
+    Y[i] = mad_lo_cc(m, FpConst::P(1), Y[i]);
+    Y[i + 1] = madc_hi_cc(m, FpConst::P(1), Y[i + 1]);
+#pragma unroll
+    for (int j = 3; j < NL; j += 2) {
+      Y[i + j - 1] = madc_lo_cc(m, FpConst::P(j), Y[i + j - 1]);
+      Y[i + j] = madc_hi_cc(m, FpConst::P(j), Y[i + j]);
+    }
+    Y[i + NL] = addc(0, 0);
+    if (i == 0) {
+      c = 0;
+    } else {
+      uint32_t t = add_cc(X[i], Y[i - 1]);
+      uint32_t c1 = addc(0, 0);
+      t = add_cc(t, c);
+      c = addc(c1, 0);
+      (void)t;
+    }
+  }
+  r[0] = add_cc(X[NL], Y[NL - 1]);
+#pragma unroll
+  for (int k = 1; k < NL; k++) r[k] = addc_cc(X[NL + k], Y[NL - 1 + k]);
+  r[0] = add_cc(r[0], c);
+#pragma unroll
+  for (int k = 1; k < NL; k++) r[k] = addc_cc(r[k], 0);
+  r[0] = add_cc(r[0], T[NL]);
+#pragma unroll
+  for (int k = 1; k < NL; k++) r[k] = addc_cc(r[k], T[NL + k]);
+  if (STRICT) cond_sub<false>(r);
+}
+
+// ---------------------------------------------------------------------------
 // Field element API
 // ---------------------------------------------------------------------------
 struct Fp {
@@ -339,7 +456,11 @@ struct Fp {
     mont_mul_raw<true>(r.v, a.v, b.v);
     return r;
   }
-  GM_DEVI static fp_t sqr(const fp_t &a) { return mul(a, a); }
+  GM_DEVI static fp_t sqr(const fp_t &a) {
+    fp_t r;
+    mont_sqr_raw<true>(r.v, a.v);
+    return r;
+  }
   GM_DEVI static fp_t to_mont(const fp_t &a) {
     fp_t r2;
 #pragma unroll
@@ -386,7 +507,20 @@ static __device__ __noinline__ fp_t fp_mul_call(fp_t a, fp_t b) {
   mont_mul_raw<true>(r.v, a.v, b.v);
   return r;
 }
+static __device__ __noinline__ fp_t fp_sqr_call(fp_t a) {
+  fp_t r;
+  mont_sqr_raw<true>(r.v, a.v);
+  return r;
+}
 struct FpOut : Fp {
+  GM_DEVI static fp_t mul(const fp_t &a, const fp_t &b) { return fp_mul_call(a, b); }
+  GM_DEVI static fp_t sqr(const fp_t &a) { return fp_sqr_call(a); }
+};
+// The bucket-accumulation loop squares through the general product: with a
+// second ~900-instruction out-of-line function its loop no longer stays in
+// the instruction cache, which costs more than the squaring saves (measured
+// on B200: 13.68 ms against 13.30 ms for the G1 2^20 accumulation).
+struct FpOutMulOnly : Fp {
   GM_DEVI static fp_t mul(const fp_t &a, const fp_t &b) { return fp_mul_call(a, b); }
   GM_DEVI static fp_t sqr(const fp_t &a) { return fp_mul_call(a, a); }
 };

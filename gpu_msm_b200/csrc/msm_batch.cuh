@@ -22,9 +22,10 @@ struct BatchClassPlan {
   int count = 0;        // MSMs in this class
   int64_t P = 0;        // points in this class
   int64_t K = 0, nb = 0, nthreads = 0;
-  int L1 = 8, FAN = 4, nseg = 0;
+  RedLayout rl;
+  int64_t long_cap = 0;
   size_t o_counts = 0, o_offsets = 0, o_bsum = 0, o_entries = 0, o_buckets = 0, o_head = 0, o_tail = 0, o_hk = 0,
-         o_tk = 0, o_red[3] = {0, 0, 0}, o_err = 0;
+         o_tk = 0, o_longq = 0, o_err = 0;
   size_t ws_bytes = 0;
   char *ws = nullptr;       // workspace (owned)
   char *desc = nullptr;     // point_start | base_off | sc_off | out_index (owned)
@@ -54,9 +55,6 @@ void batch_class_layout(BatchClassPlan &cp, int limbs, int sms, int dev) {
   cp.nthreads = (int64_t)sms * acc_blocks_per_sm<F>(dev) * ACC_THREADS;
   const int64_t max_entries = cp.P * cp.dp.W;
   if (cp.nthreads > max_entries) cp.nthreads = std::max<int64_t>(1, (max_entries + 127) / 128 * 128);
-  cp.L1 = std::min(8, cp.dp.B);
-  cp.nseg = (cp.dp.B + cp.L1 - 1) / cp.L1;
-  const int64_t red = (int64_t)cp.count * cp.dp.W * cp.nseg;
   Carve cv;
   cp.o_counts = cv.take<uint32_t>(cp.K);
   cp.o_offsets = cv.take<uint32_t>(cp.K + 1);
@@ -67,9 +65,11 @@ void batch_class_layout(BatchClassPlan &cp, int limbs, int sms, int dev) {
   cp.o_tail = cv.take<xyzz_t<F>>(cp.nthreads);
   cp.o_hk = cv.take<int32_t>(cp.nthreads);
   cp.o_tk = cv.take<int32_t>(cp.nthreads);
-  cp.o_red[0] = cv.take<xyzz_t<F>>(red);
-  cp.o_red[1] = cv.take<xyzz_t<F>>((red + cp.FAN - 1) / cp.FAN + (int64_t)cp.count * cp.dp.W);
-  cp.o_red[2] = cv.take<xyzz_t<F>>((red + cp.FAN - 1) / cp.FAN + (int64_t)cp.count * cp.dp.W);
+  cp.rl.plan<F>((int64_t)cp.count * cp.dp.W, cp.dp.B, (int64_t)sms * level0_blocks_per_sm<F>(dev) * 128, cv);
+  cp.rl.sms = sms;
+  cp.rl.dev = dev;
+  cp.long_cap = cp.nthreads / FIX_SHORT + 1;
+  cp.o_longq = cv.take<int32_t>((size_t)(1 + cp.long_cap));
   cp.o_err = cv.take<uint32_t>(4);
   cp.ws_bytes = cv.off;
 }
@@ -90,8 +90,7 @@ int batch_class_run(const BatchPlan &plan, const BatchClassPlan &cp, cudaStream_
   auto *hk = (int32_t *)(ws + cp.o_hk);
   auto *tk = (int32_t *)(ws + cp.o_tk);
   auto *err = (uint32_t *)(ws + cp.o_err);
-  xyzz_t<F> *red[3];
-  for (int k = 0; k < 3; k++) red[k] = (xyzz_t<F> *)(ws + cp.o_red[k]);
+  auto *long_q = (int32_t *)(ws + cp.o_longq);
   MultiDesc md;
   md.point_start = (const int64_t *)cp.desc;
   md.base_off = md.point_start + cp.count + 1;
@@ -102,6 +101,7 @@ int batch_class_run(const BatchPlan &plan, const BatchClassPlan &cp, cudaStream_
   int launches = 0;
   GM_CHECK(cudaMemsetAsync(counts, 0, cp.K * sizeof(uint32_t), s));
   GM_CHECK(cudaMemsetAsync(err, 0, sizeof(uint32_t), s));
+  GM_CHECK(cudaMemsetAsync(long_q, 0, sizeof(int32_t), s));
   k_count_multi<<<grid_for(cp.P, 256), 256, 0, s>>>(scalars, plan.bases, Rec<F>::U4, F::LIMBS, cp.P, md, cp.dp,
                                                     counts);
   GM_CHECK_LAUNCH("k_count_multi");
@@ -116,26 +116,16 @@ int batch_class_run(const BatchPlan &plan, const BatchClassPlan &cp, cudaStream_
   k_accumulate<F><<<grid_for(cp.nthreads, ACC_THREADS), ACC_THREADS, acc_smem_bytes<F>(), s>>>(
       plan.bases, entries, offsets, cp.K, cp.nthreads, buckets, head, tail, hk, tk);
   GM_CHECK_LAUNCH("k_accumulate");
-  k_fixup<F><<<grid_for(cp.nthreads, 128), 128, 0, s>>>(offsets, cp.K, cp.nthreads, buckets, head, tail, hk, tk, err);
-  GM_CHECK_LAUNCH("k_fixup");
-  const int Wtot = cp.count * cp.dp.W;
-  k_reduce_segments<F><<<grid_for((int64_t)Wtot * cp.nseg, 128), 128, 0, s>>>(buckets, offsets, Wtot, cp.dp.B, cp.L1,
-                                                                             red[0]);
-  GM_CHECK_LAUNCH("k_reduce_segments");
-  launches += 3;
-  int N = cp.nseg, pong = 1;
-  xyzz_t<F> *src = red[0];
-  while (N > 1) {
-    const int nout = (N + cp.FAN - 1) / cp.FAN;
-    k_tree_sum<F><<<grid_for((int64_t)Wtot * nout, 128), 128, 0, s>>>(src, Wtot, N, cp.FAN, red[pong]);
-    GM_CHECK_LAUNCH("k_tree_sum");
-    launches++;
-    src = red[pong];
-    pong = pong == 1 ? 2 : 1;
-    N = nout;
-  }
-  k_combine_indexed<F><<<grid_for(cp.count, 32), 32, 0, s>>>(src, cp.count, cp.dp.W, cp.c, out_index, results);
-  GM_CHECK_LAUNCH("k_combine_indexed");
+  launches++;
+  int rc = fixup_launch<F>(s, offsets, cp.K, cp.nthreads, buckets, head, tail, hk, tk, err, long_q, cp.long_cap,
+                           &launches);
+  if (rc) return rc;
+  const xyzz_t<F> *src = nullptr;
+  rc = reduce_launch<F>(s, cp.rl, buckets, offsets, ws, &src, &launches);
+  if (rc) return rc;
+  k_combine_quad<F><<<grid_for(4 * (int64_t)cp.count, 128), 128, 0, s>>>(src, cp.count, cp.dp.W, cp.c, out_index,
+                                                                          results);
+  GM_CHECK_LAUNCH("k_combine_quad");
   launches++;
   count_launches(launches);
   return GM_OK;

@@ -11,6 +11,7 @@
 
 #include "msm_engine.h"
 #include "msm_kernels.cuh"
+#include "msm_reduce.cuh"
 
 namespace gm {
 
@@ -50,12 +51,21 @@ struct MsmLayout {
   int FAN = 4;    // fan-in of the segment-share tree
   int nseg = 0;   // reduction segments per window
   size_t o_counts, o_offsets, o_bsum, o_entries, o_buckets, o_head, o_tail, o_hk, o_tk, o_red[3], o_err, o_packed;
+  size_t o_longq = 0;
   size_t bytes = 0;
   int64_t nb = 0;
   int64_t red_elems = 0;
+  int64_t long_cap = 0;
   bool need_pack = false;
+  // leveled reduction (k_red_level0/1 + quad tree) and split fix-up; the
+  // allocation-free entry point keeps the segment reduction
+  bool leveled = false;
+  RedLayout rl;
 
-  void plan(int64_t n_, int limbs, int c, int sms, int acc_blocks_per_sm, bool pack) {
+  // level0_wave: threads of k_red_level0 resident at once (leveled only)
+  void plan(int64_t n_, int limbs, int c, int sms, int acc_blocks_per_sm, bool pack, bool leveled_ = false,
+            int64_t level0_wave = 0) {
+    leveled = leveled_;
     n = n_;
     need_pack = pack;
     dp.c = c;
@@ -81,9 +91,17 @@ struct MsmLayout {
     o_tail = cv.take<xyzz_t<F>>(nthreads);
     o_hk = cv.take<int32_t>(nthreads);
     o_tk = cv.take<int32_t>(nthreads);
-    o_red[0] = cv.take<xyzz_t<F>>(red_elems);
-    o_red[1] = cv.take<xyzz_t<F>>((red_elems + FAN - 1) / FAN + dp.W);
-    o_red[2] = cv.take<xyzz_t<F>>((red_elems + FAN - 1) / FAN + dp.W);
+    if (leveled) {
+      rl.plan<F>(dp.W, dp.B, level0_wave, cv);
+      rl.sms = sms;
+      long_cap = nthreads / FIX_SHORT + 1;
+      o_longq = cv.take<int32_t>((size_t)(1 + long_cap));
+      o_red[0] = o_red[1] = o_red[2] = 0;
+    } else {
+      o_red[0] = cv.take<xyzz_t<F>>(red_elems);
+      o_red[1] = cv.take<xyzz_t<F>>((red_elems + FAN - 1) / FAN + dp.W);
+      o_red[2] = cv.take<xyzz_t<F>>((red_elems + FAN - 1) / FAN + dp.W);
+    }
     o_err = cv.take<uint32_t>(4);
     o_packed = pack ? cv.take<uint4>((size_t)n * Rec<F>::U4) : 0;
     bytes = cv.off;
@@ -111,6 +129,72 @@ static int acc_blocks_per_sm(int dev) {
 
 static inline unsigned grid_for(int64_t n, int block) { return (unsigned)((n + block - 1) / block); }
 
+// Resident blocks per SM of the level-0 reduction kernel (cached per device).
+template <class F>
+static int level0_blocks_per_sm(int dev) {
+  static std::mutex mu;
+  static int cached[64] = {0};
+  std::lock_guard<std::mutex> lk(mu);
+  if (dev < 0 || dev >= 64) dev = 0;
+  if (cached[dev] == 0) {
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_red_level0<F>, 128, 0) != cudaSuccess) b = 1;
+    cached[dev] = std::max(1, b);
+  }
+  return cached[dev];
+}
+
+// Split fix-up: short runs serially, long runs by a block-level tree.
+// long_q[0] must be zero on entry.
+template <class F>
+int fixup_launch(cudaStream_t s, const uint32_t *offsets, int64_t K, int64_t nthreads, xyzz_t<F> *buckets,
+                 const xyzz_t<F> *head, const xyzz_t<F> *tail, const int32_t *hk, const int32_t *tk, uint32_t *err,
+                 int32_t *long_q, int64_t long_cap, int *launches) {
+  k_fixup_split<F><<<grid_for(nthreads, 128), 128, 0, s>>>(offsets, K, nthreads, buckets, head, tail, hk, tk, err,
+                                                            long_q, long_cap);
+  GM_CHECK_LAUNCH("k_fixup_split");
+  k_fixup_long<F><<<FIX_LONG_BLOCKS, 128, 0, s>>>(offsets, K, nthreads, buckets, head, tail, hk, err, long_q,
+                                                   long_cap);
+  GM_CHECK_LAUNCH("k_fixup_long");
+  *launches += 2;
+  return GM_OK;
+}
+
+// Leveled bucket reduction over rl.G groups of rl.B buckets; *sums receives
+// the G window sums (contiguous).
+template <class F>
+int reduce_launch(cudaStream_t s, const RedLayout &rl, const xyzz_t<F> *buckets, const uint32_t *offsets, char *ws,
+                  const xyzz_t<F> **sums, int *launches) {
+  auto *X = (xyzz_t<F> *)(ws + rl.o_X);
+  auto *A0 = (xyzz_t<F> *)(ws + rl.o_A0);
+  const int64_t wave = (int64_t)rl.sms * level0_blocks_per_sm<F>(rl.dev);
+  const int64_t blocks0 = std::min<int64_t>(wave, (rl.G * rl.nseg0 + 127) / 128);
+  k_red_level0<F><<<(unsigned)std::max<int64_t>(1, blocks0), 128, 0, s>>>(buckets, offsets, rl.G, rl.B, rl.L0,
+                                                                           rl.nseg0, X, rl.M, A0);
+  GM_CHECK_LAUNCH("k_red_level0");
+  (*launches)++;
+  if (rl.nseg1 > 0) {
+    k_red_level1<F><<<grid_for(4 * rl.G * rl.nseg1, 128), 128, 0, s>>>(A0, rl.G, rl.nseg0, rl.L1, rl.nseg1,
+                                                                        rl.L0, X, rl.M);
+    GM_CHECK_LAUNCH("k_red_level1");
+    (*launches)++;
+  }
+  const xyzz_t<F> *src = X;
+  int N = rl.M, k = 0;
+  while (N > 1) {
+    const int nout = (N + RedLayout::FAN - 1) / RedLayout::FAN;
+    auto *dst = (xyzz_t<F> *)(ws + rl.o_t[k]);
+    k_tree_quad<F><<<grid_for(4 * rl.G * nout, 128), 128, 0, s>>>(src, rl.G, N, RedLayout::FAN, dst);
+    GM_CHECK_LAUNCH("k_tree_quad");
+    (*launches)++;
+    src = dst;
+    k ^= 1;
+    N = nout;
+  }
+  *sums = src;
+  return GM_OK;
+}
+
 // Runs the whole pipeline.  bases: packed records (or null to pack from
 // ref_points), scalars: device u64 limbs, out: reference projective layout.
 template <class F>
@@ -135,7 +219,9 @@ int msm_launch(cudaStream_t s, int dev, const uint4 *bases, const uint64_t *ref_
     return GM_ERR_ARG;
   }
   MsmLayout<F> lay;
-  lay.plan(n, limbs, c, sms, acc_blocks_per_sm<F>(dev), bases == nullptr);
+  lay.plan(n, limbs, c, sms, acc_blocks_per_sm<F>(dev), bases == nullptr, /*leveled=*/true,
+           (int64_t)sms * level0_blocks_per_sm<F>(dev) * 128);
+  lay.rl.dev = dev;
   if ((uint64_t)n * lay.dp.W >= (1ull << 32)) {
     set_last_error("too many (point, window) entries for 32-bit offsets");
     return GM_ERR_ARG;
@@ -154,9 +240,6 @@ int msm_launch(cudaStream_t s, int dev, const uint4 *bases, const uint64_t *ref_
   auto *hk = (int32_t *)(ws + lay.o_hk);
   auto *tk = (int32_t *)(ws + lay.o_tk);
   auto *err = (uint32_t *)(ws + lay.o_err);
-  xyzz_t<F> *red[3];
-  for (int k = 0; k < 3; k++) red[k] = (xyzz_t<F> *)(ws + lay.o_red[k]);
-
   profile_mark(s, "start");
   int launches = 0;
   if (bases == nullptr) {
@@ -169,6 +252,8 @@ int msm_launch(cudaStream_t s, int dev, const uint4 *bases, const uint64_t *ref_
   }
   GM_CHECK(cudaMemsetAsync(counts, 0, lay.K * sizeof(uint32_t), s));
   GM_CHECK(cudaMemsetAsync(err, 0, sizeof(uint32_t), s));
+  auto *long_q = (int32_t *)(ws + lay.o_longq);
+  GM_CHECK(cudaMemsetAsync(long_q, 0, sizeof(int32_t), s));
   k_count<<<grid_for(n, 256), 256, 0, s>>>(scalars, bases, Rec<F>::U4, F::LIMBS, n, lay.dp, counts);
   GM_CHECK_LAUNCH("k_count");
   k_scan_blocksum<<<(unsigned)lay.nb, SCAN_THREADS, 0, s>>>(counts, lay.K, bsum);
@@ -185,32 +270,16 @@ int msm_launch(cudaStream_t s, int dev, const uint4 *bases, const uint64_t *ref_
   GM_CHECK_LAUNCH("k_accumulate");
   launches++;
   profile_mark(s, "accumulate");
-  k_fixup<F><<<grid_for(lay.nthreads, 128), 128, 0, s>>>(offsets, lay.K, lay.nthreads, buckets, head, tail, hk, tk, err);
-  GM_CHECK_LAUNCH("k_fixup");
-  launches++;
+  rc = fixup_launch<F>(s, offsets, lay.K, lay.nthreads, buckets, head, tail, hk, tk, err, long_q, lay.long_cap,
+                       &launches);
+  if (rc) return rc;
   profile_mark(s, "fixup");
 
-  // bucket reduction: per-segment shares, then a fan-in tree per window
+  // bucket reduction: leveled running sums, then a quad fan-in tree
   const int W = lay.dp.W;
-  {
-    const int64_t th = (int64_t)W * lay.nseg;
-    k_reduce_segments<F><<<grid_for(th, 128), 128, 0, s>>>(buckets, offsets, W, lay.dp.B, lay.L1, red[0]);
-    GM_CHECK_LAUNCH("k_reduce_segments");
-    launches++;
-  }
-  int N = lay.nseg;
-  xyzz_t<F> *src = red[0];
-  int pong = 1;
-  while (N > 1) {
-    const int nout = (N + lay.FAN - 1) / lay.FAN;
-    xyzz_t<F> *dst = red[pong];
-    k_tree_sum<F><<<grid_for((int64_t)W * nout, 128), 128, 0, s>>>(src, W, N, lay.FAN, dst);
-    GM_CHECK_LAUNCH("k_tree_sum");
-    launches++;
-    src = dst;
-    pong = pong == 1 ? 2 : 1;
-    N = nout;
-  }
+  const xyzz_t<F> *src = nullptr;
+  rc = reduce_launch<F>(s, lay.rl, buckets, offsets, ws, &src, &launches);
+  if (rc) return rc;
   profile_mark(s, "reduce");
   // window combination: the serial Horner tail runs on the host (lower
   // latency per product) unless the stream is being captured into a graph
@@ -220,8 +289,8 @@ int msm_launch(cudaStream_t s, int dev, const uint4 *bases, const uint64_t *ref_
     rc = enqueue_host_tail(s, F::LIMBS == NL ? 1 : 2, src, W, c, out_proj);
     if (rc) return rc;
   } else {
-    k_combine<F><<<1, 32, 0, s>>>(src, 1, W, c, out_proj);
-    GM_CHECK_LAUNCH("k_combine");
+    k_combine_quad<F><<<1, 32, 0, s>>>(src, 1, W, c, nullptr, out_proj);
+    GM_CHECK_LAUNCH("k_combine_quad");
     launches++;
   }
   profile_mark(s, "combine");

@@ -56,6 +56,18 @@ struct OutOfLine<Fp2> {
   using type = Fp2Out;
 };
 
+// Policy of the accumulation loop (one out-of-line product only).
+template <class F>
+struct AccPolicy;
+template <>
+struct AccPolicy<Fp> {
+  using type = FpOutMulOnly;
+};
+template <>
+struct AccPolicy<Fp2> {
+  using type = Fp2Out;
+};
+
 template <class A, class B>
 GM_DEVI xyzz_t<A> as_xyzz(const xyzz_t<B> &p) {
   return xyzz_t<A>{p.X, p.Y, p.ZZ, p.ZZZ};
@@ -426,7 +438,7 @@ __global__ void __launch_bounds__(ACC_THREADS) k_accumulate(const uint4 *__restr
                                                     xyzz_t<F> *__restrict__ part_head, xyzz_t<F> *__restrict__ part_tail,
                                                     int32_t *__restrict__ head_key, int32_t *__restrict__ tail_key) {
   using T = typename F::T;
-  using FA = typename OutOfLine<F>::type;
+  using FA = typename AccPolicy<F>::type;
   constexpr int CH = F::LIMBS / 2;  // 16-byte chunks of x || y
   extern __shared__ uint4 stage_mem[];  // [2][CH][ACC_THREADS], acc_smem_bytes<F>()
   auto stage = reinterpret_cast<uint4(*)[CH][ACC_THREADS]>(stage_mem);

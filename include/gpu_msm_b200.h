@@ -186,10 +186,14 @@ int gm_msm_default_window(int group, int64_t n, int scalar_limbs);
  *   batched form of fp_mont_mul (src/fp.cu:370).
  * gm_fp_mul_array: c[i] = a[i]*b[i] mod p on standard-form values, the
  *   C-ABI form of fp_mul_array_device (include/fp_kernels.h:39).
+ * gm_fp_mont_sqr_array: c[i] = a[i]^2*R^-1, the dedicated Montgomery squaring
+ *   used inside the point formulas (same result as fp_mont_mul(a, a),
+ *   src/fp.cu:370; the reference has no separate squaring).
  * gm_fp2_mont_mul_array: batched fp2_mont_mul (src/fp2.cu:88).
  * gm_fp2_mul_array: batched normal-form fp2_mul on device pointers, the
  *   device-resident form of fp2_mul_array_host (include/fp2_kernels.h:19). */
 int gm_fp_mont_mul_array(gm_stream_t stream, uint32_t gpu_index, Fp *d_c, const Fp *d_a, const Fp *d_b, int64_t n);
+int gm_fp_mont_sqr_array(gm_stream_t stream, uint32_t gpu_index, Fp *d_c, const Fp *d_a, int64_t n);
 int gm_fp_mul_array(gm_stream_t stream, uint32_t gpu_index, Fp *d_c, const Fp *d_a, const Fp *d_b, int64_t n);
 int gm_fp2_mont_mul_array(gm_stream_t stream, uint32_t gpu_index, Fp2 *d_c, const Fp2 *d_a, const Fp2 *d_b, int64_t n);
 int gm_fp2_mul_array(gm_stream_t stream, uint32_t gpu_index, Fp2 *d_c, const Fp2 *d_a, const Fp2 *d_b, int64_t n);

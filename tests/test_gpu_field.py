@@ -102,3 +102,18 @@ def test_fp_mont_mul_matches_reference_host(cuda):
     ref.ref_fp_mont_mul_batch(ctypes.c_void_p(want.ctypes.data), ctypes.c_void_p(a.ctypes.data),
                               ctypes.c_void_p(b.ctypes.data), ctypes.c_int64(len(a)))
     assert np.array_equal(run("fp_mont_mul", a, b, cuda), want)
+
+
+def test_fp_mont_sqr_matches_mul(cuda):
+    """The dedicated squaring equals fp_mont_mul(a, a) of the oracle on edge
+    values and seeded random elements."""
+    import torch
+    P = pyref.P
+    edge = [0, 1, 2, 3, P - 1, P - 2, P - 3, (1 << 448) % P, 1 << 445, (1 << 446) - 1 if (1 << 446) - 1 < P else P - 5,
+            P >> 1, (P >> 1) + 1, (1 << 447) % P, (1 << 32) - 1, (1 << 224) - 1]
+    rng = random.Random(7)
+    edge += [rng.randrange(P) for _ in range(4096)]
+    a = oracle.ints_to_fp_array(edge)
+    out = gm.field_sqr_array(dev(a, cuda).reshape(len(edge), -1))
+    torch.cuda.synchronize()
+    assert np.array_equal(host(out).reshape(a.shape), oracle.fp_mont_mul(a, a))

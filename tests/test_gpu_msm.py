@@ -238,3 +238,50 @@ def test_concurrent_streams(cuda):
     torch.cuda.synchronize()
     for o, w in zip(outs, wants):
         assert oracle.same_point(oracle.proj_to_affine(gm.to_numpy_proj(o, 1), 1), w)
+
+
+@pytest.mark.parametrize("group,n,c", [(1, 3000, 0), (1, 3000, 8), (1, 5000, 3), (2, 1000, 0)])
+def test_heavy_buckets(cuda, group, n, c):
+    """Most scalars equal to 1 or 2: a few buckets hold thousands of entries
+    and span many accumulation slices (the long-run fix-up path)."""
+    rng = np.random.default_rng(n + c)
+    sc = wl.make_scalars(n, seed=n + 7 * c + group)
+    pick = rng.random(n)
+    sc[pick < 0.6] = 0
+    sc[pick < 0.6, 0] = 1
+    sc[(pick >= 0.6) & (pick < 0.8)] = 0
+    sc[(pick >= 0.6) & (pick < 0.8), 0] = 2
+    logs = wl.make_base_logs(n, seed=n + 11 * c + group)
+    pts = make_bases(logs, group, cuda)
+    want = oracle.generator_multiple(wl.expected_log(sc, logs), group=group)
+    assert oracle.same_point(device_msm(pts, sc, group, cuda, c=c), want)
+
+
+def test_plain_msm_graph_capture(cuda):
+    """A plain MSM captured into a CUDA graph (device-side window combination)
+    and replayed with new scalars."""
+    import torch
+    n = 3000
+    logs = wl.make_base_logs(n, seed=77)
+    pts = make_bases(logs, 1, cuda)
+    sc0 = wl.make_scalars(n, seed=78)
+    static_sc = t_dev(sc0, cuda).reshape(n, -1).clone()
+    out = torch.zeros((1, gm.G1P_WORDS), dtype=torch.int64, device=cuda)
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        gm.msm_device(pts, static_sc, group=1, out=out, stream=s)
+    torch.cuda.current_stream().wait_stream(s)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, capture_error_mode="thread_local"):
+        gm.msm_device(pts, static_sc, group=1, out=out)
+    for seed in (79, 80):
+        sc = wl.make_scalars(n, seed=seed)
+        static_sc.copy_(t_dev(sc, cuda).reshape(n, -1))
+        out.zero_()
+        g.replay()
+        torch.cuda.synchronize()
+        got = oracle.proj_to_affine(gm.to_numpy_proj(out, 1), 1)
+        assert oracle.same_point(got, oracle.generator_multiple(wl.expected_log(sc, logs)))
+    del g
