@@ -55,7 +55,8 @@ C_API = [
     "g1_msm_limbs_wrapper", "g2_msm_limbs_wrapper", "gm_g1_msm_device", "gm_g2_msm_device",
     "gm_g1_msm_device_c", "gm_g2_msm_device_c", "gm_msm_default_window",
     "gm_fp_mont_mul_array", "gm_fp_mul_array", "gm_fp2_mont_mul_array", "gm_fp2_mul_array",
-    "gm_fp_mont_sqr_array",
+    "gm_fp_mont_sqr_array", "gm_fp_add_array", "gm_fp2_add_array",
+    "gm_g1_msm_device_affine", "gm_g2_msm_device_affine",
     "gm_g1_to_montgomery_batch", "gm_g2_to_montgomery_batch",
     "gm_g1_generator_mul_batch", "gm_g2_generator_mul_batch", "gm_last_error",
     "gm_profile_enable", "gm_profile_collect", "gm_launch_count_reset", "gm_imad_probe",
@@ -87,10 +88,13 @@ def lib() -> ctypes.CDLL:
             getattr(L, name).argtypes = [vp, vp, vp, i32, i32, u32, i32]
         for name in ("gm_g1_msm_device", "gm_g2_msm_device"):
             getattr(L, name).argtypes = [vp, u32, vp, vp, vp, i32, i32]
+        for name in ("gm_g1_msm_device_affine", "gm_g2_msm_device_affine"):
+            getattr(L, name).argtypes = [vp, u32, vp, vp, vp, i32, i32]
         for name in ("gm_g1_msm_device_c", "gm_g2_msm_device_c"):
             getattr(L, name).argtypes = [vp, u32, vp, vp, vp, i32, i32, i32]
         L.gm_msm_default_window.argtypes = [i32, i64, i32]
-        for name in ("gm_fp_mont_mul_array", "gm_fp_mul_array", "gm_fp2_mont_mul_array", "gm_fp2_mul_array"):
+        for name in ("gm_fp_mont_mul_array", "gm_fp_mul_array", "gm_fp2_mont_mul_array", "gm_fp2_mul_array",
+                     "gm_fp_add_array", "gm_fp2_add_array"):
             getattr(L, name).argtypes = [vp, u32, vp, vp, vp, i64]
         L.gm_fp_mont_sqr_array.argtypes = [vp, u32, vp, vp, i64]
         for name in ("gm_g1_to_montgomery_batch", "gm_g2_to_montgomery_batch"):
@@ -304,6 +308,24 @@ def msm_device(points, scalars, group: int = 1, window_bits: int = 0, out=None, 
     return out
 
 
+def msm_device_affine(points, scalars, group: int = 1, out=None, stream=None):
+    """MSM with an affine result (reference layout, Montgomery form, infinity
+    flag), the device form of point_msm_async<G1Point>/<G2Point>.  Returns an
+    int64 tensor of G1_WORDS / G2_WORDS words."""
+    import torch
+    _require(points, G1_WORDS if group == 1 else G2_WORDS, "points")
+    n = points.shape[0]
+    _require(scalars, None, "scalars", rows=n)
+    limbs = scalars.shape[1]
+    words = G1_WORDS if group == 1 else G2_WORDS
+    if out is None:
+        out = torch.empty(words, dtype=torch.int64, device=points.device)
+    fn = lib().gm_g1_msm_device_affine if group == 1 else lib().gm_g2_msm_device_affine
+    _check(fn(_stream_handle(stream), _dev_index(points), ctypes.c_void_p(out.data_ptr()),
+              ctypes.c_void_p(points.data_ptr()), ctypes.c_void_p(scalars.data_ptr()), limbs, n), "msm_device_affine")
+    return out
+
+
 NOALLOC_MAX_POINTS = 4096
 
 
@@ -375,7 +397,8 @@ def to_montgomery_batch(points, group: int = 1, stream=None):
 
 def field_mul_array(a, b, op: str = "fp_mont_mul", out=None, stream=None):
     """Element-wise field products on device tensors of shape (n, 7) [Fp] or
-    (n, 14) [Fp2], int64.  op: fp_mont_mul | fp_mul | fp2_mont_mul | fp2_mul."""
+    (n, 14) [Fp2], int64.  op: fp_mont_mul | fp_mul | fp_add | fp2_mont_mul | fp2_mul |
+    fp2_add."""
     import torch
     cols = 7 if op.startswith("fp_") else 14
     _require(a, cols, "a")

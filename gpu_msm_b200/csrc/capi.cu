@@ -437,6 +437,81 @@ int gm_g2_msm_device_c(gm_stream_t stream, uint32_t gpu_index, G2ProjectivePoint
                                  scalar_limbs, n, (uint64_t *)d_result, window_bits, nullptr);
 }
 
+}  // extern "C"
+
+namespace {
+
+// Projective sum -> affine result on the host, ordered on the stream: the
+// pinned slot holds the projective input at offset 0 and the affine output
+// at AFF_OFF.
+constexpr size_t AFF_OFF = 512;
+
+void CUDART_CB g1_to_affine_cb(void *slot) {
+  auto *base = static_cast<char *>(slot);
+  projective_to_affine_g1_wrapper(reinterpret_cast<G1Point *>(base + AFF_OFF),
+                                  reinterpret_cast<const G1ProjectivePoint *>(base));
+}
+void CUDART_CB g2_to_affine_cb(void *slot) {
+  auto *base = static_cast<char *>(slot);
+  projective_to_affine_g2_wrapper(reinterpret_cast<G2Point *>(base + AFF_OFF),
+                                  reinterpret_cast<const G2ProjectivePoint *>(base));
+}
+
+template <class F, class Aff, class Prj>
+int msm_affine(gm_stream_t stream, uint32_t gpu_index, Aff *d_result, const Aff *d_points, const uint64_t *d_scalars,
+               int scalar_limbs, int n, cudaHostFn_t to_affine) {
+  if (d_result == nullptr || n < 0 || (n > 0 && (d_points == nullptr || d_scalars == nullptr))) return gm::GM_ERR_ARG;
+  int rc = gm::select_device(gpu_index);
+  if (rc) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (n == 0) {
+    Aff inf;
+    memset(&inf, 0, sizeof(inf));
+    inf.infinity = true;
+    void *slot = nullptr;
+    rc = gm::pinned_acquire(&slot);
+    if (rc) return rc;
+    memcpy(slot, &inf, sizeof(inf));
+    cudaError_t e = cudaMemcpyAsync(d_result, slot, sizeof(Aff), cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return gm::record_error(e, "msm_affine copy");
+    return gm::enqueue_pinned_release(s, slot);
+  }
+  void *tmp = nullptr;
+  rc = gm::pool_alloc((int)gpu_index, s, sizeof(Prj), &tmp);
+  if (rc) return rc;
+  rc = gm::msm_launch<F>(s, (int)gpu_index, nullptr, (const uint64_t *)d_points, 0, d_scalars, scalar_limbs, n,
+                         (uint64_t *)tmp, 0, nullptr);
+  if (rc) return rc;
+  void *slot = nullptr;
+  rc = gm::pinned_acquire(&slot);
+  if (rc) return rc;
+  cudaError_t e = cudaMemcpyAsync(slot, tmp, sizeof(Prj), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaLaunchHostFunc(s, to_affine, slot);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(d_result, static_cast<char *>(slot) + AFF_OFF, sizeof(Aff), cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return gm::record_error(e, "msm_affine");
+  rc = gm::enqueue_pinned_release(s, slot);
+  if (rc) return rc;
+  e = cudaFreeAsync(tmp, s);
+  return e == cudaSuccess ? gm::GM_OK : gm::record_error(e, "msm_affine free");
+}
+
+}  // namespace
+
+extern "C" {
+
+int gm_g1_msm_device_affine(gm_stream_t stream, uint32_t gpu_index, G1Point *d_result, const G1Point *d_points,
+                            const uint64_t *d_scalars, int scalar_limbs, int n) {
+  return msm_affine<gm::Fp, G1Point, G1ProjectivePoint>(stream, gpu_index, d_result, d_points, d_scalars, scalar_limbs,
+                                                        n, g1_to_affine_cb);
+}
+
+int gm_g2_msm_device_affine(gm_stream_t stream, uint32_t gpu_index, G2Point *d_result, const G2Point *d_points,
+                            const uint64_t *d_scalars, int scalar_limbs, int n) {
+  return msm_affine<gm::Fp2, G2Point, G2ProjectivePoint>(stream, gpu_index, d_result, d_points, d_scalars,
+                                                         scalar_limbs, n, g2_to_affine_cb);
+}
+
 int gm_g1_msm_device(gm_stream_t stream, uint32_t gpu_index, G1ProjectivePoint *d_result, const G1Point *d_points,
                      const uint64_t *d_scalars, int scalar_limbs, int n) {
   return gm_g1_msm_device_c(stream, gpu_index, d_result, d_points, d_scalars, scalar_limbs, n, 0);

@@ -15,7 +15,7 @@
 
 namespace {
 
-enum Op { MONT_MUL = 0, NORMAL_MUL = 1, MONT_SQR = 2 };
+enum Op { MONT_MUL = 0, NORMAL_MUL = 1, MONT_SQR = 2, ADD = 3 };
 
 template <class F, int OP>
 __global__ void __launch_bounds__(256) k_field_mul(uint64_t *__restrict__ c, const uint64_t *__restrict__ a,
@@ -27,6 +27,9 @@ __global__ void __launch_bounds__(256) k_field_mul(uint64_t *__restrict__ c, con
     typename F::T z;
     if constexpr (OP == MONT_SQR) {
       z = F::sqr(x);
+    } else if constexpr (OP == ADD) {
+      gm::load_ref<F>(y, b + i * Hw);
+      z = F::add(x, y);
     } else {
       gm::load_ref<F>(y, b + i * Hw);
       z = F::mul(x, y);
@@ -135,6 +138,12 @@ int gm_fp_mont_mul_array(gm_stream_t stream, uint32_t gpu_index, Fp *d_c, const 
 }
 int gm_fp_mont_sqr_array(gm_stream_t stream, uint32_t gpu_index, Fp *d_c, const Fp *d_a, int64_t n) {
   return launch_field<gm::Fp, MONT_SQR>(stream, gpu_index, d_c, d_a, d_a, n);
+}
+int gm_fp_add_array(gm_stream_t stream, uint32_t gpu_index, Fp *d_c, const Fp *d_a, const Fp *d_b, int64_t n) {
+  return launch_field<gm::Fp, ADD>(stream, gpu_index, d_c, d_a, d_b, n);
+}
+int gm_fp2_add_array(gm_stream_t stream, uint32_t gpu_index, Fp2 *d_c, const Fp2 *d_a, const Fp2 *d_b, int64_t n) {
+  return launch_field<gm::Fp2, ADD>(stream, gpu_index, d_c, d_a, d_b, n);
 }
 int gm_fp_mul_array(gm_stream_t stream, uint32_t gpu_index, Fp *d_c, const Fp *d_a, const Fp *d_b, int64_t n) {
   return launch_field<gm::Fp, NORMAL_MUL>(stream, gpu_index, d_c, d_a, d_b, n);

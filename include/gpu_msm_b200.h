@@ -32,20 +32,11 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include "gpu_msm_b200_types.h"
+
 #ifdef __cplusplus
 extern "C" {
 #endif
-
-/* Types: byte-compatible with include/fp.h:13, include/fp2.h:10 and
- * include/curve.h:13-43 of the reference (sizes 56/112/120/232/168/336 B). */
-typedef struct Fp { uint64_t limb[7]; } Fp;
-typedef struct Fp2 { Fp c0; Fp c1; } Fp2;
-typedef struct G1Point { Fp x; Fp y; bool infinity; } G1Point;
-typedef struct G2Point { Fp2 x; Fp2 y; bool infinity; } G2Point;
-typedef struct G1ProjectivePoint { Fp X; Fp Y; Fp Z; } G1ProjectivePoint;
-typedef struct G2ProjectivePoint { Fp2 X; Fp2 Y; Fp2 Z; } G2ProjectivePoint;
-
-typedef struct CUstream_st *gm_stream_t; /* a cudaStream_t */
 
 /* ======================================================================== */
 /* Part 1: the reference C-ABI (rust-api/include/rust_wrapper.h)             */
@@ -87,7 +78,9 @@ void fp_to_montgomery_wrapper(Fp *result, const Fp *value);
 /* include/curve.h:108 (src/curve.cu:833); bound with C linkage by
  * rust-api/src/ffi.rs:67.  Kept for link compatibility: the generators are
  * compile-time constants here, so this only validates the device index. */
+#ifndef GM_CXX_API_IMPL /* the C++-linkage twin is in gpu_msm_b200_cxx.h */
 void init_device_generators(gm_stream_t stream, uint32_t gpu_index);
+#endif
 
 /* ======================================================================== */
 /* Part 2: additive entry points                                             */
@@ -119,6 +112,16 @@ int gm_g1_msm_device_c(gm_stream_t stream, uint32_t gpu_index, G1ProjectivePoint
                        const uint64_t *d_scalars, int scalar_limbs, int n, int window_bits);
 int gm_g2_msm_device_c(gm_stream_t stream, uint32_t gpu_index, G2ProjectivePoint *d_result, const G2Point *d_points,
                        const uint64_t *d_scalars, int scalar_limbs, int n, int window_bits);
+
+/* MSM with an affine result (Montgomery form; infinity flag set for the
+ * identity), the device form of point_msm_async<G1Point>/<G2Point>
+ * (include/curve.h:238, src/curve.cu:2763), which returns an affine point.
+ * Asynchronous: the projective sum is converted to affine by a host
+ * function ordered on the stream.  n == 0 writes the point at infinity. */
+int gm_g1_msm_device_affine(gm_stream_t stream, uint32_t gpu_index, G1Point *d_result, const G1Point *d_points,
+                            const uint64_t *d_scalars, int scalar_limbs, int n);
+int gm_g2_msm_device_affine(gm_stream_t stream, uint32_t gpu_index, G2Point *d_result, const G2Point *d_points,
+                            const uint64_t *d_scalars, int scalar_limbs, int n);
 
 /* G1 MSM that allocates nothing.  No counterpart in the reference.  For
  * callers that cannot allocate device memory per call: frameworks that hand
@@ -194,6 +197,11 @@ int gm_msm_default_window(int group, int64_t n, int scalar_limbs);
  *   device-resident form of fp2_mul_array_host (include/fp2_kernels.h:19). */
 int gm_fp_mont_mul_array(gm_stream_t stream, uint32_t gpu_index, Fp *d_c, const Fp *d_a, const Fp *d_b, int64_t n);
 int gm_fp_mont_sqr_array(gm_stream_t stream, uint32_t gpu_index, Fp *d_c, const Fp *d_a, int64_t n);
+/* c[i] = a[i] + b[i] mod p (either form); the device form of
+ * fp_add_array_device (include/fp_kernels.h:33) and fp2_add_array_host
+ * (include/fp2_kernels.h:13). */
+int gm_fp_add_array(gm_stream_t stream, uint32_t gpu_index, Fp *d_c, const Fp *d_a, const Fp *d_b, int64_t n);
+int gm_fp2_add_array(gm_stream_t stream, uint32_t gpu_index, Fp2 *d_c, const Fp2 *d_a, const Fp2 *d_b, int64_t n);
 int gm_fp_mul_array(gm_stream_t stream, uint32_t gpu_index, Fp *d_c, const Fp *d_a, const Fp *d_b, int64_t n);
 int gm_fp2_mont_mul_array(gm_stream_t stream, uint32_t gpu_index, Fp2 *d_c, const Fp2 *d_a, const Fp2 *d_b, int64_t n);
 int gm_fp2_mul_array(gm_stream_t stream, uint32_t gpu_index, Fp2 *d_c, const Fp2 *d_a, const Fp2 *d_b, int64_t n);

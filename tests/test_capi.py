@@ -34,6 +34,18 @@ def test_library_exports_every_declared_symbol():
     assert set(gm.C_API) <= set(declared)
 
 
+def test_library_exports_reference_cxx_api():
+    """Every mangled symbol of the reference's C++ MSM-path API (fixture made
+    from the reference's own headers by golden/make_cxx_symbols.py) resolves
+    in the library, so objects built against the reference's headers link."""
+    L = gm.lib()
+    path = os.path.join(ROOT, "tests", "golden", "cxx_symbols.txt")
+    syms = [s.strip() for s in open(path) if s.strip() and not s.startswith("#")]
+    assert len(syms) >= 20
+    missing = [s for s in syms if not hasattr(L, s)]
+    assert not missing, missing
+
+
 def test_struct_sizes():
     assert (gm.G1.itemsize, gm.G2.itemsize, gm.G1P.itemsize, gm.G2P.itemsize) == (120, 232, 168, 336)
 
