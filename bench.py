@@ -41,6 +41,10 @@ FP_MICRO = 1 << 26
 METRIC = "MSM points/s (G1 2^20, G2 2^18) batched vs plain on 1 B200, bit-exact; p99 ms"
 
 
+# fixed-base window tables (window widths) for the resident-table workloads
+PRECOMPUTE_BATCH = (8, 10, 12, 14)
+PRECOMPUTE_SERVE = {1: (11, 20), 2: (11, 16)}
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -390,11 +394,17 @@ def measure_serving(gm, wl, dev, loads=(0.5, 1.0, 2.0), count=120):
     import torch
 
     from gpu_msm_b200 import serving
-    tables = {}
+    tables, served_tables, build_s = {}, {}, 0.0
     for g, log2n, seed in ((1, 20, 8181), (2, 18, 8282)):
         logs = wl.make_base_logs(1 << log2n, seed=seed)
         pts = gm.generator_mul_batch(torch.from_numpy(logs.view(np.int64)).to(dev), group=g)
         tables[g] = gm.ResidentBases(pts, group=g)
+        # the server's copy carries fixed-base window tables
+        served_tables[g] = gm.ResidentBases(pts, group=g)
+        t0 = time.perf_counter()
+        for c in PRECOMPUTE_SERVE[g]:
+            served_tables[g].precompute(c)
+        build_s += time.perf_counter() - t0
         del pts
     pool = wl.make_scalars(1 << 21, seed=8383)
     ranges = {1: (10, 20), 2: (10, 18)}
@@ -412,11 +422,13 @@ def measure_serving(gm, wl, dev, loads=(0.5, 1.0, 2.0), count=120):
     t, g, sizes, scs = trace(1e9, 1)
     plain_lat, _, span = serving.plain_trace(tables, np.zeros(24), g[:24], scs[:24], dev)
     capacity = 24 / span
-    res = {"plain_capacity_req_s": capacity, "requests_per_load": count, "loads": []}
+    res = {"plain_capacity_req_s": capacity, "requests_per_load": count,
+           "window_tables": {f"g{g}": list(v) for g, v in PRECOMPUTE_SERVE.items()}, "table_build_s": build_s,
+           "loads": []}
     for k, load in enumerate(loads):
         rate = load * capacity
         t, g, sizes, scs = trace(rate, 100 + k)
-        server = serving.MsmServer(tables, max_batch=64, max_points=1 << 22, slots=2).start()
+        server = serving.MsmServer(served_tables, max_batch=64, max_points=1 << 22, slots=2).start()
         reqs, span_s = serving.serve_trace(server, t, g, scs)
         server.stop()
         lat_p, outs_p, span_p = serving.plain_trace(tables, t, g, scs, dev)
@@ -429,7 +441,7 @@ def measure_serving(gm, wl, dev, loads=(0.5, 1.0, 2.0), count=120):
                        "batches": len(batch_sizes), "mean_batch": float(np.mean(batch_sizes))},
             "plain": {"points_per_s": pts / span_p, **serving.percentiles(lat_p)},
             "sampled_results_equal": ok})
-    for tb in tables.values():
+    for tb in list(tables.values()) + list(served_tables.values()):
         tb.close()
     return res
 
@@ -489,19 +501,58 @@ def measure_batched(gm, wl, dev, count=512, table_log2=16):
     e1.record()
     torch.cuda.synchronize()
     t_seq = e0.elapsed_time(e1) / 1e3
-    # canonical equality of every output (projective forms may differ)
-    a = gm.to_numpy_proj(out, 1)
+    # canonical equality of sampled outputs (projective forms may differ)
     b_ = gm.to_numpy_proj(seq_out, 1)
-    same = all(np.array_equal(gm.projective_to_affine(a[i:i + 1], 1)["x"], gm.projective_to_affine(b_[i:i + 1], 1)["x"])
-               for i in range(0, count, 37))
+
+    def same_as_seq(o):
+        a = gm.to_numpy_proj(o, 1)
+        return all(np.array_equal(gm.projective_to_affine(a[i:i + 1], 1)["x"],
+                                  gm.projective_to_affine(b_[i:i + 1], 1)["x"]) for i in range(0, count, 37))
+
     res = {"count": count, "points": total, "classes": plan.classes(),
            "batched_points_per_s": total / t_batch, "batched_ms": t_batch * 1e3,
            "sequential_points_per_s": total / t_seq, "sequential_ms": t_seq * 1e3,
-           "speedup": t_seq / t_batch, "sampled_outputs_equal": same, "graph": "cuda graph replay"}
+           "speedup": t_seq / t_batch, "sampled_outputs_equal": same_as_seq(out), "graph": "cuda graph replay"}
     del g
+    plan.close()
+    # the same batch over fixed-base window tables of the resident set
+    t0 = time.perf_counter()
+    for c in PRECOMPUTE_BATCH:
+        table.precompute(c)
+    t_pre = time.perf_counter() - t0
+    plan = gm.BatchPlan(table, sizes)
+    out_pc = torch.empty_like(out)
+    t_pc = time_graph(plan, sc, out_pc)
+    res["precomputed"] = {"windows": list(PRECOMPUTE_BATCH), "classes": plan.classes(),
+                          "build_s": t_pre, "batched_points_per_s": total / t_pc, "batched_ms": t_pc * 1e3,
+                          "speedup_vs_sequential": t_seq / t_pc, "sampled_outputs_equal": same_as_seq(out_pc)}
     plan.close()
     table.close()
     return res
+
+
+def time_graph(plan, sc, out, reps=5):
+    """Capture plan.run in a CUDA graph and time its replays (seconds)."""
+    import torch
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        plan.run(sc, out=out)
+    torch.cuda.current_stream().wait_stream(s)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, capture_error_mode="thread_local"):
+        plan.run(sc, out=out)
+    g.replay()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        g.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    del g
+    return e0.elapsed_time(e1) / reps / 1e3
 
 
 def main():

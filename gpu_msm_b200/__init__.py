@@ -61,7 +61,7 @@ C_API = [
     "gm_g1_generator_mul_batch", "gm_g2_generator_mul_batch", "gm_last_error",
     "gm_profile_enable", "gm_profile_collect", "gm_launch_count_reset", "gm_imad_probe",
     "gm_g1_sum_projective", "gm_g2_sum_projective", "gm_g1_msm_device_noalloc",
-    "gm_bases_create", "gm_bases_destroy", "gm_bases_count", "gm_msm_resident", "gm_batch_plan_create",
+    "gm_bases_create", "gm_bases_destroy", "gm_bases_count", "gm_bases_precompute", "gm_msm_resident", "gm_batch_plan_create",
     "gm_batch_plan_run", "gm_batch_plan_destroy", "gm_batch_plan_bytes", "gm_batch_plan_classes",
     "gm_batch_run", "gm_batch_workspace_bytes", "gm_g1_sum_projective_host",
 ]
@@ -112,6 +112,7 @@ def lib() -> ctypes.CDLL:
         L.gm_g1_msm_device_noalloc.argtypes = [vp, u32, vp, vp, vp, i32, i32]
         L.gm_bases_create.argtypes = [u32, i32, vp, i64, i32, vp]
         L.gm_bases_destroy.argtypes = [vp]
+        L.gm_bases_precompute.argtypes = [vp, i32, i32]
         L.gm_bases_count.argtypes = [vp]
         L.gm_bases_count.restype = i64
         L.gm_msm_resident.argtypes = [vp, vp, i64, i32, vp, i32, vp, i32]
@@ -491,6 +492,24 @@ class ResidentBases:
         _check(lib().gm_bases_create(_dev_index(points), group, ctypes.c_void_p(points.data_ptr()), self.n,
                                      1 if montgomery else 0, ctypes.byref(h)), "gm_bases_create")
         self.handle = h
+        self.precomputed = []   # window widths with a fixed-base table
+
+    def precompute(self, window_bits: int, scalar_limbs: int = 5):
+        """Build the fixed-base window table for window width window_bits
+        (``gm_bases_precompute``): 2^(c w) * P_i for every window, so MSMs of
+        that width need one bucket set and no window doublings.  Blocks."""
+        _check(lib().gm_bases_precompute(self.handle, int(window_bits), int(scalar_limbs)), "gm_bases_precompute")
+        if window_bits not in self.precomputed:
+            self.precomputed.append(int(window_bits))
+        return self
+
+    def windows_for(self, sizes, scalar_limbs: int = 5):
+        """Per-MSM window widths to pass to a plan: 0 (the library picks the
+        cheapest fixed-base table) when the set has tables, else the tuned
+        widths."""
+        if self.precomputed:
+            return [0] * len(sizes)
+        return [tuned_window(self.group, int(s), scalar_limbs) for s in sizes]
 
     def msm(self, scalars, offset: int = 0, n: int = None, window_bits: int = 0, out=None, stream=None):
         """Asynchronous MSM over entries [offset, offset + n)."""
@@ -562,7 +581,7 @@ class BatchPlan:
         self.limbs = scalar_limbs
         offs = None if base_offsets is None else np.ascontiguousarray(base_offsets, dtype=np.int64)
         if window_bits is None:
-            window_bits = [tuned_window(bases.group, int(s), scalar_limbs) for s in self.sizes]
+            window_bits = bases.windows_for(self.sizes, scalar_limbs)
         wins = np.ascontiguousarray(window_bits, dtype=np.int32)
         h = ctypes.c_void_p()
         _check(lib().gm_batch_plan_create(bases.handle, scalar_limbs, self.count, _p(self.sizes),
@@ -612,7 +631,7 @@ def batch_run(bases: ResidentBases, sizes, scalars, base_offsets=None, window_bi
     total = int(sizes.sum())
     _require(scalars, None, "scalars", rows=total)
     if window_bits is None:
-        window_bits = [tuned_window(bases.group, int(s), scalars.shape[1]) for s in sizes]
+        window_bits = bases.windows_for(sizes, scalars.shape[1])
     wins = np.ascontiguousarray(window_bits, dtype=np.int32)
     offs = None if base_offsets is None else np.ascontiguousarray(base_offsets, dtype=np.int64)
     words = G1P_WORDS if bases.group == 1 else G2P_WORDS
@@ -627,7 +646,7 @@ def batch_run(bases: ResidentBases, sizes, scalars, base_offsets=None, window_bi
 def batch_workspace_bytes(bases: ResidentBases, sizes, window_bits=None, scalar_limbs: int = 5) -> int:
     sizes = np.ascontiguousarray(sizes, dtype=np.int64)
     if window_bits is None:
-        window_bits = [tuned_window(bases.group, int(s), scalar_limbs) for s in sizes]
+        window_bits = bases.windows_for(sizes, scalar_limbs)
     wins = np.ascontiguousarray(window_bits, dtype=np.int32)
     v = int(lib().gm_batch_workspace_bytes(bases.handle, scalar_limbs, len(sizes), _p(sizes), _p(wins)))
     if v < 0:

@@ -22,6 +22,8 @@ extern template int batch_layouts<Fp>(BatchPlan &, int);
 extern template int batch_layouts<Fp2>(BatchPlan &, int);
 extern template int batch_run<Fp>(const BatchPlan &, cudaStream_t, const uint64_t *, uint64_t *);
 extern template int batch_run<Fp2>(const BatchPlan &, cudaStream_t, const uint64_t *, uint64_t *);
+extern template int window_table_launch<Fp>(cudaStream_t, const uint4 *, int64_t, int, int, uint4 *);
+extern template int window_table_launch<Fp2>(cudaStream_t, const uint4 *, int64_t, int, int, uint4 *);
 }  // namespace gm
 
 struct gm_bases {
@@ -29,6 +31,19 @@ struct gm_bases {
   int dev = 0;
   int64_t n = 0;
   uint4 *packed = nullptr;  // owned, Rec<F>::U4 uint4 per point
+  // fixed-base window tables (gm_bases_precompute): record w*n + i holds
+  // 2^(c w) * point i, w < W
+  struct WindowTable {
+    int c = 0, W = 0;
+    uint4 *table = nullptr;  // owned
+  };
+  std::vector<WindowTable> tables;
+
+  const WindowTable *table_for(int c, int W) const {
+    for (const auto &t : tables)
+      if (t.c == c && t.W >= W) return &t;
+    return nullptr;
+  }
 };
 
 struct gm_batch_plan {
@@ -66,8 +81,22 @@ int build_classes(const gm_bases *b, int scalar_limbs, int count, const int64_t 
       return gm::GM_ERR_ARG;
     }
     sc_row[i + 1] = sc_row[i] + sizes[i];
-    const int c =
-        window_bits && window_bits[i] > 0 ? window_bits[i] : gm::default_window(b->group, sizes[i], scalar_limbs);
+    int c = window_bits && window_bits[i] > 0 ? window_bits[i] : 0;
+    if (c == 0 && !b->tables.empty()) {
+      // with fixed-base tables an MSM costs ~10 products per (point, non-zero
+      // window) plus 2 additions (28 products) per bucket of its single
+      // bucket set; take the cheapest table
+      double best = 0;
+      for (const auto &t : b->tables) {
+        if (t.W < gm::windows_for(t.c, scalar_limbs)) continue;
+        const double cost = 10.0 * (double)sizes[i] * (64.0 * scalar_limbs / t.c) + 28.0 * (double)(1 << (t.c - 1));
+        if (c == 0 || cost < best) {
+          best = cost;
+          c = t.c;
+        }
+      }
+    }
+    if (c == 0) c = gm::default_window(b->group, sizes[i], scalar_limbs);
     if (c < 2 || c > 20) {
       gm::set_last_error("window width out of range");
       return gm::GM_ERR_ARG;
@@ -86,6 +115,10 @@ int build_classes(const gm_bases *b, int scalar_limbs, int count, const int64_t 
     cp.c = kv.first;
     cp.count = (int)kv.second.size();
     for (int i : kv.second) cp.P += sizes[i];
+    if (const auto *t = b->table_for(cp.c, gm::windows_for(cp.c, scalar_limbs))) {
+      cp.pc_table = t->table;
+      cp.pc_stride = b->n;
+    }
     plan.classes.push_back(cp);
   }
   int sms = 0;
@@ -166,7 +199,42 @@ int gm_bases_destroy(gm_bases *b) {
   if (!b) return gm::GM_OK;
   cudaSetDevice(b->dev);
   cudaFree(b->packed);
+  for (auto &t : b->tables) cudaFree(t.table);
   delete b;
+  return gm::GM_OK;
+}
+
+int gm_bases_precompute(gm_bases *b, int window_bits, int scalar_limbs) {
+  if (!b || window_bits < 2 || window_bits > 20 || scalar_limbs < 1 || scalar_limbs > gm::MAX_SCALAR_LIMBS)
+    return gm::GM_ERR_ARG;
+  const int W = gm::windows_for(window_bits, scalar_limbs);
+  if (b->table_for(window_bits, W)) return gm::GM_OK;
+  if ((uint64_t)b->n * W >= (1ull << 31)) {
+    gm::set_last_error("window table too large for 31-bit record indices");
+    return gm::GM_ERR_ARG;
+  }
+  int rc = gm::select_device((uint32_t)b->dev);
+  if (rc) return rc;
+  const int u4 = b->group == 1 ? gm::Rec<gm::Fp>::U4 : gm::Rec<gm::Fp2>::U4;
+  gm_bases::WindowTable t;
+  t.c = window_bits;
+  t.W = W;
+  cudaError_t e = cudaMalloc(&t.table, (size_t)b->n * W * u4 * sizeof(uint4));
+  if (e != cudaSuccess) {
+    gm::record_error(e, "cudaMalloc(window table)");
+    return gm::GM_ERR_ALLOC;
+  }
+  rc = b->group == 1 ? gm::window_table_launch<gm::Fp>(nullptr, b->packed, b->n, window_bits, W, t.table)
+                     : gm::window_table_launch<gm::Fp2>(nullptr, b->packed, b->n, window_bits, W, t.table);
+  if (rc == gm::GM_OK) {
+    e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) rc = gm::record_error(e, "k_window_table");
+  }
+  if (rc) {
+    cudaFree(t.table);
+    return rc;
+  }
+  b->tables.push_back(t);
   return gm::GM_OK;
 }
 
@@ -179,6 +247,13 @@ int gm_msm_resident(gm_stream_t stream, const gm_bases *b, int64_t base_offset, 
     return gm::GM_ERR_ARG;
   int rc = gm::select_device((uint32_t)b->dev);
   if (rc) return rc;
+  if (!b->tables.empty() && n > 0) {
+    // fixed-base tables: a batch of one (single bucket set, no window doublings)
+    const int64_t size = n;
+    const int32_t wb = window_bits;
+    return gm_batch_run(stream, b, scalar_limbs, 1, &size, &base_offset, window_bits > 0 ? &wb : nullptr, d_scalars,
+                        d_result);
+  }
   if (b->group == 1)
     return gm::msm_launch<gm::Fp>((cudaStream_t)stream, b->dev, b->packed + base_offset * gm::Rec<gm::Fp>::U4, nullptr,
                                   0, d_scalars, scalar_limbs, n, (uint64_t *)d_result, window_bits, nullptr);

@@ -24,6 +24,9 @@ struct BatchClassPlan {
   int64_t K = 0, nb = 0, nthreads = 0;
   RedLayout rl;
   int64_t long_cap = 0;
+  // fixed-base window table (precomputed mode): record w*pc_stride + base
+  const uint4 *pc_table = nullptr;
+  int64_t pc_stride = 0;
   size_t o_counts = 0, o_offsets = 0, o_bsum = 0, o_entries = 0, o_buckets = 0, o_head = 0, o_tail = 0, o_hk = 0,
          o_tk = 0, o_longq = 0, o_err = 0;
   size_t ws_bytes = 0;
@@ -50,7 +53,9 @@ void batch_class_layout(BatchClassPlan &cp, int limbs, int sms, int dev) {
   cp.dp.W = windows_for(cp.c, limbs);
   cp.dp.B = 1 << (cp.c - 1);
   cp.dp.limbs = limbs;
-  cp.K = (int64_t)cp.count * cp.dp.W * cp.dp.B;
+  // precomputed mode: one bucket set per MSM (no window index in the key)
+  const int64_t groups = (int64_t)cp.count * (cp.pc_stride ? 1 : cp.dp.W);
+  cp.K = groups * cp.dp.B;
   cp.nb = (cp.K + SCAN_TILE - 1) / SCAN_TILE;
   cp.nthreads = (int64_t)sms * acc_blocks_per_sm<F>(dev) * ACC_THREADS;
   const int64_t max_entries = cp.P * cp.dp.W;
@@ -65,7 +70,7 @@ void batch_class_layout(BatchClassPlan &cp, int limbs, int sms, int dev) {
   cp.o_tail = cv.take<xyzz_t<F>>(cp.nthreads);
   cp.o_hk = cv.take<int32_t>(cp.nthreads);
   cp.o_tk = cv.take<int32_t>(cp.nthreads);
-  cp.rl.plan<F>((int64_t)cp.count * cp.dp.W, cp.dp.B, (int64_t)sms * level0_blocks_per_sm<F>(dev) * 128, cv);
+  cp.rl.plan<F>(groups, cp.dp.B, (int64_t)sms * level0_blocks_per_sm<F>(dev) * 128, cv);
   cp.rl.sms = sms;
   cp.rl.dev = dev;
   cp.long_cap = cp.nthreads / FIX_SHORT + 1;
@@ -103,18 +108,18 @@ int batch_class_run(const BatchPlan &plan, const BatchClassPlan &cp, cudaStream_
   GM_CHECK(cudaMemsetAsync(err, 0, sizeof(uint32_t), s));
   GM_CHECK(cudaMemsetAsync(long_q, 0, sizeof(int32_t), s));
   k_count_multi<<<grid_for(cp.P, 256), 256, 0, s>>>(scalars, plan.bases, Rec<F>::U4, F::LIMBS, cp.P, md, cp.dp,
-                                                    counts);
+                                                    cp.pc_stride, counts);
   GM_CHECK_LAUNCH("k_count_multi");
   k_scan_blocksum<<<(unsigned)cp.nb, SCAN_THREADS, 0, s>>>(counts, cp.K, bsum);
   k_scan_top<<<1, SCAN_THREADS, 0, s>>>(bsum, (int)cp.nb);
   k_scan_final<<<(unsigned)cp.nb, SCAN_THREADS, 0, s>>>(counts, cp.K, bsum, offsets);
   GM_CHECK_LAUNCH("k_scan");
   k_scatter_multi<<<grid_for(cp.P, 256), 256, 0, s>>>(scalars, plan.bases, Rec<F>::U4, F::LIMBS, cp.P, md, cp.dp,
-                                                      offsets, counts, entries);
+                                                      cp.pc_stride, offsets, counts, entries);
   GM_CHECK_LAUNCH("k_scatter_multi");
   launches += 5;
   k_accumulate<F><<<grid_for(cp.nthreads, ACC_THREADS), ACC_THREADS, acc_smem_bytes<F>(), s>>>(
-      plan.bases, entries, offsets, cp.K, cp.nthreads, buckets, head, tail, hk, tk);
+      cp.pc_table ? cp.pc_table : plan.bases, entries, offsets, cp.K, cp.nthreads, buckets, head, tail, hk, tk);
   GM_CHECK_LAUNCH("k_accumulate");
   launches++;
   int rc = fixup_launch<F>(s, offsets, cp.K, cp.nthreads, buckets, head, tail, hk, tk, err, long_q, cp.long_cap,
@@ -123,11 +128,21 @@ int batch_class_run(const BatchPlan &plan, const BatchClassPlan &cp, cudaStream_
   const xyzz_t<F> *src = nullptr;
   rc = reduce_launch<F>(s, cp.rl, buckets, offsets, ws, &src, &launches);
   if (rc) return rc;
-  k_combine_quad<F><<<grid_for(4 * (int64_t)cp.count, 128), 128, 0, s>>>(src, cp.count, cp.dp.W, cp.c, out_index,
-                                                                          results);
+  // precomputed mode: one window per MSM, so the combination is a conversion
+  k_combine_quad<F><<<grid_for(4 * (int64_t)cp.count, 128), 128, 0, s>>>(src, cp.count, cp.pc_stride ? 1 : cp.dp.W,
+                                                                          cp.c, out_index, results);
   GM_CHECK_LAUNCH("k_combine_quad");
   launches++;
   count_launches(launches);
+  return GM_OK;
+}
+
+// Builds the fixed-base window table of n packed points: W windows of c bits.
+template <class F>
+int window_table_launch(cudaStream_t s, const uint4 *packed, int64_t n, int c, int W, uint4 *table) {
+  k_window_table<F><<<grid_for(n, 128), 128, 0, s>>>(packed, n, c, W, table);
+  GM_CHECK_LAUNCH("k_window_table");
+  count_launches(1);
   return GM_OK;
 }
 

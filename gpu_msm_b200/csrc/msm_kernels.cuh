@@ -103,6 +103,23 @@ GM_DEVI void load_base(typename F::T &x, typename F::T &y, const uint4 *rec) {
   }
 }
 
+// Store x, y and the infinity word as one packed record (pad words zero).
+template <class F>
+GM_DEVI void store_base(uint4 *dst, typename F::T &x, typename F::T &y, uint32_t inf) {
+  constexpr int L = F::LIMBS;
+  uint32_t w[4 * Rec<F>::U4];
+#pragma unroll
+  for (int k = 0; k < 4 * Rec<F>::U4; k++) w[k] = 0;
+#pragma unroll
+  for (int k = 0; k < L; k++) {
+    w[k] = limb_ref<F>(x, k);
+    w[L + k] = limb_ref<F>(y, k);
+  }
+  w[2 * L] = inf;
+#pragma unroll
+  for (int q = 0; q < Rec<F>::U4; q++) dst[q] = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
+}
+
 GM_DEVI uint32_t base_is_inf(const uint4 *rec, int u4_per_rec, int limbs) {
   const uint32_t *w = reinterpret_cast<const uint32_t *>(rec);
   return __ldg(w + 2 * limbs);
@@ -170,18 +187,47 @@ __global__ void k_pack_ref(uint4 *__restrict__ out, const uint64_t *__restrict__
     x = field_to_mont<F>(x);
     y = field_to_mont<F>(y);
   }
-  uint32_t w[4 * Rec<F>::U4];
-#pragma unroll
-  for (int k = 0; k < 4 * Rec<F>::U4; k++) w[k] = 0;
-#pragma unroll
-  for (int k = 0; k < L; k++) {
-    w[k] = limb_ref<F>(x, k);
-    w[L + k] = limb_ref<F>(y, k);
+  store_base<F>(out + i * Rec<F>::U4, x, y, inf ? 1u : 0u);
+}
+
+// Fixed-base window table of a resident base set: record (w, i) at index
+// w*n + i holds 2^(c w) P_i in affine Montgomery form (w = 0 is P_i), so an
+// MSM over the set needs one bucket set for all windows and no window
+// doublings.  One thread per point: c XYZZ doublings per window, then the
+// affine conversion with one field inversion.
+template <class F>
+__global__ void __launch_bounds__(128) k_window_table(const uint4 *__restrict__ packed, int64_t n, int c, int W,
+                                                      uint4 *__restrict__ table) {
+  using FA = typename OutOfLine<F>::type;
+  using T = typename F::T;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint4 *rec = packed + i * Rec<F>::U4;
+  T x, y;
+  load_base<F>(x, y, rec);
+  if (base_is_inf(rec, Rec<F>::U4, F::LIMBS)) {
+    for (int w = 0; w < W; w++) store_base<F>(table + ((int64_t)w * n + i) * Rec<F>::U4, x, y, 1u);
+    return;
   }
-  w[2 * L] = inf ? 1u : 0u;
-  uint4 *dst = out + i * Rec<F>::U4;
-#pragma unroll
-  for (int q = 0; q < Rec<F>::U4; q++) dst[q] = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
+  store_base<F>(table + i * Rec<F>::U4, x, y, 0u);
+  xyzz_t<FA> acc;
+  acc.X = x;
+  acc.Y = y;
+  acc.ZZ = F::one();
+  acc.ZZZ = F::one();
+  for (int w = 1; w < W; w++) {
+    for (int k = 0; k < c; k++) xyzz_dbl_cold<FA>(acc);
+    uint4 *dst = table + ((int64_t)w * n + i) * Rec<F>::U4;
+    if (xyzz_is_inf(acc)) {
+      T z = F::zero();
+      store_base<F>(dst, z, z, 1u);
+      continue;
+    }
+    const T I = F::inv(FA::mul(acc.ZZ, acc.ZZZ));
+    T ax = FA::mul(acc.X, FA::mul(I, acc.ZZZ));
+    T ay = FA::mul(acc.Y, FA::mul(I, acc.ZZ));
+    store_base<F>(dst, ax, ay, 0u);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -256,6 +302,9 @@ static __global__ void k_scatter(const uint64_t *__restrict__ scalars, const uin
 // base_off[i] + j of the shared table and scalar row sc_off[i] + j.  Its
 // bucket keys are i*W*B + w*B + |d|-1, so one counting sort, one
 // accumulation and one reduction serve every MSM of the batch.
+// With a fixed-base window table (pc_stride = table points n > 0) the window
+// index moves from the bucket key to the base record: keys are i*B + |d|-1
+// and the entry addresses record w*n + base of the table.
 struct MultiDesc {
   const int64_t *point_start;  // [count + 1]
   const int64_t *base_off;     // [count]
@@ -277,34 +326,35 @@ GM_DEVI int msm_of(const int64_t *__restrict__ ps, int count, int64_t p) {
 
 static __global__ void k_count_multi(const uint64_t *__restrict__ scalars, const uint4 *__restrict__ bases,
                                      int rec_u4, int field_limbs, int64_t P, MultiDesc md, DigitParams dp,
-                                     uint32_t *__restrict__ counts) {
+                                     int64_t pc_stride, uint32_t *__restrict__ counts) {
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P) return;
   const int i = msm_of(md.point_start, md.count, p);
   const int64_t j = p - __ldg(md.point_start + i);
   const int64_t bi = __ldg(md.base_off + i) + j;
   if (base_is_inf(bases + bi * rec_u4, rec_u4, field_limbs)) return;
-  const int64_t kbase = (int64_t)i * dp.W * dp.B;
+  const int64_t kbase = (int64_t)i * (pc_stride ? 1 : dp.W) * dp.B;
   for_each_digit(scalars + (__ldg(md.sc_off + i) + j) * dp.limbs, dp, [&](int w, int d) {
-    atomicAdd(&counts[kbase + (int64_t)w * dp.B + (d < 0 ? -d : d) - 1], 1u);
+    atomicAdd(&counts[kbase + (pc_stride ? 0 : (int64_t)w * dp.B) + (d < 0 ? -d : d) - 1], 1u);
   });
 }
 
 static __global__ void k_scatter_multi(const uint64_t *__restrict__ scalars, const uint4 *__restrict__ bases,
                                        int rec_u4, int field_limbs, int64_t P, MultiDesc md, DigitParams dp,
-                                       const uint32_t *__restrict__ offsets, uint32_t *__restrict__ counts,
-                                       uint32_t *__restrict__ entries) {
+                                       int64_t pc_stride, const uint32_t *__restrict__ offsets,
+                                       uint32_t *__restrict__ counts, uint32_t *__restrict__ entries) {
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P) return;
   const int i = msm_of(md.point_start, md.count, p);
   const int64_t j = p - __ldg(md.point_start + i);
   const int64_t bi = __ldg(md.base_off + i) + j;
   if (base_is_inf(bases + bi * rec_u4, rec_u4, field_limbs)) return;
-  const int64_t kbase = (int64_t)i * dp.W * dp.B;
+  const int64_t kbase = (int64_t)i * (pc_stride ? 1 : dp.W) * dp.B;
   for_each_digit(scalars + (__ldg(md.sc_off + i) + j) * dp.limbs, dp, [&](int w, int d) {
-    const int64_t key = kbase + (int64_t)w * dp.B + (d < 0 ? -d : d) - 1;
+    const int64_t key = kbase + (pc_stride ? 0 : (int64_t)w * dp.B) + (d < 0 ? -d : d) - 1;
     const uint32_t rank = atomicSub(&counts[key], 1u) - 1u;
-    entries[offsets[key] + rank] = ((uint32_t)bi << 1) | (d < 0 ? 1u : 0u);
+    const int64_t rec = pc_stride ? (int64_t)w * pc_stride + bi : bi;
+    entries[offsets[key] + rank] = ((uint32_t)rec << 1) | (d < 0 ? 1u : 0u);
   });
 }
 

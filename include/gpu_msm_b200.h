@@ -167,6 +167,16 @@ typedef struct gm_batch_plan gm_batch_plan;
 int gm_bases_create(uint32_t gpu_index, int group, const void *d_points, int64_t n, int points_montgomery,
                     gm_bases **out);
 int gm_bases_destroy(gm_bases *bases);
+/* Fixed-base window table of a resident set: for window width c =
+ * window_bits, stores 2^(c w) * P_i for every point and every window w that
+ * scalars of scalar_limbs limbs need (64 * scalar_limbs / c + 1), in affine
+ * Montgomery form.  Afterwards MSMs over the set (gm_msm_resident, batches,
+ * plans) whose window width is c use one bucket set for all windows and no
+ * window doublings; MSMs without an explicit width pick the cheapest table.
+ * Memory: n * W records (128 B G1, 256 B G2).  Blocks until built; calling
+ * it again for a width that is already there does nothing.  No counterpart in
+ * the reference. */
+int gm_bases_precompute(gm_bases *b, int window_bits, int scalar_limbs);
 int64_t gm_bases_count(const gm_bases *bases);
 int gm_msm_resident(gm_stream_t stream, const gm_bases *bases, int64_t base_offset, int n, const uint64_t *d_scalars,
                     int scalar_limbs, void *d_result, int window_bits);

@@ -30,7 +30,7 @@ from . import pyref
 _HERE = os.path.dirname(os.path.abspath(__file__))
 
 # numpy dtypes byte-compatible with the reference structs (include/fp.h:13,
-# include/fp2.h:10, include/curve.h:13-43); see SURVEY F6 for the sizes.
+# include/fp2.h:10, include/curve.h:13-43): 56, 112, 120, 232, 168 and 336 bytes.
 FP = np.dtype(("<u8", (7,)))
 FP2 = np.dtype(("<u8", (2, 7)))
 G1 = np.dtype([("x", "<u8", (7,)), ("y", "<u8", (7,)), ("infinity", "u1"), ("_pad", "u1", (7,))])

@@ -121,3 +121,85 @@ def test_batch_g2(cuda):
     res = plan.run(t_dev(sc, cuda).reshape(-1, 5))
     torch.cuda.synchronize()
     check(res, expected(sizes, offs, sc, logs, 2), 2)
+
+
+def test_batch_precomputed_tables(cuda):
+    """Fixed-base window tables: batches whose width has a table run with one
+    bucket set per MSM; mixed with a width that has no table; results equal
+    the oracle and the plain launches."""
+    import torch
+    table, logs = make_table(1 << 11, 1, cuda, seed=71)
+    table.precompute(8).precompute(11)
+    sizes, offs, sc = batch_inputs(1 << 11, 30, 1, 11, seed=72)
+    # widths chosen by the library among the tables
+    plan = gm.BatchPlan(table, sizes, offs)
+    assert set(w for w, _ in plan.classes()) <= {8, 11}
+    res = plan.run(t_dev(sc, cuda).reshape(-1, 5))
+    torch.cuda.synchronize()
+    want = expected(sizes, offs, sc, logs, 1)
+    check(res, want, 1)
+    # explicit widths: 8 and 11 use tables, 5 does not
+    wins = np.array([[5, 8, 11][i % 3] for i in range(len(sizes))], dtype=np.int32)
+    plan2 = gm.BatchPlan(table, sizes, offs, window_bits=wins)
+    res2 = plan2.run(t_dev(sc, cuda).reshape(-1, 5))
+    torch.cuda.synchronize()
+    check(res2, want, 1)
+    # single resident MSM through the table
+    sc_d = t_dev(sc, cuda).reshape(-1, 5)
+    one = table.msm(sc_d[:int(sizes[0])], offset=int(offs[0]))
+    torch.cuda.synchronize()
+    assert oracle.same_point(oracle.proj_to_affine(gm.to_numpy_proj(one, 1), 1), want[0])
+    # graph capture and replay with new scalars
+    static_sc = sc_d.clone()
+    out = torch.empty((len(sizes), gm.G1P_WORDS), dtype=torch.int64, device=cuda)
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        plan.run(static_sc, out=out)
+    torch.cuda.current_stream().wait_stream(s)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, capture_error_mode="thread_local"):
+        plan.run(static_sc, out=out)
+    new = wl.make_scalars(int(sizes.sum()), seed=73)
+    static_sc.copy_(t_dev(new, cuda).reshape(-1, 5))
+    g.replay()
+    torch.cuda.synchronize()
+    check(out, expected(sizes, offs, new, logs, 1), 1)
+    del g
+
+
+def test_batch_precomputed_heavy_and_infinity(cuda):
+    """Precomputed tables with infinity bases in the set and scalars that put
+    thousands of entries into a few buckets."""
+    import torch
+    n = 1 << 10
+    logs = wl.make_base_logs(n, seed=81)
+    pts = gm.generator_mul_batch(t_dev(logs, cuda), group=1)
+    host = gm.to_numpy_points(pts, 1).copy()
+    host["infinity"][::7] = 1
+    table = gm.ResidentBases(t_dev(host, cuda).reshape(n, -1), group=1)
+    table.precompute(9)
+    sizes = np.array([n, 500, 77], dtype=np.int64)
+    offs = np.array([0, 100, 900], dtype=np.int64)
+    sc = wl.make_scalars(int(sizes.sum()), seed=82)
+    sc[: n // 2] = 0
+    sc[: n // 2, 0] = 1
+    res = gm.batch_run(table, sizes, t_dev(sc, cuda).reshape(-1, 5), base_offsets=offs)
+    torch.cuda.synchronize()
+    got = gm.to_numpy_proj(res, 1)
+    row = 0
+    for i, (s_, o) in enumerate(zip(sizes, offs)):
+        want = oracle.msm_pippenger(host[o:o + s_], sc[row:row + s_], group=1)
+        assert oracle.same_point(oracle.proj_to_affine(got[i:i + 1], 1), want), i
+        row += s_
+
+
+def test_batch_precomputed_g2(cuda):
+    import torch
+    table, logs = make_table(1 << 9, 2, cuda, seed=91)
+    table.precompute(7)
+    sizes, offs, sc = batch_inputs(1 << 9, 8, 2, 9, seed=92)
+    res = gm.BatchPlan(table, sizes, offs).run(t_dev(sc, cuda).reshape(-1, 5))
+    torch.cuda.synchronize()
+    check(res, expected(sizes, offs, sc, logs, 2), 2)
