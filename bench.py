@@ -248,8 +248,8 @@ def run_ours(args, rank, world, local_rank):
     if rank != 0:
         return
 
-    # IMAD ceilings of this GPU (project microbenchmark): the lo/hi mix of a
-    # Montgomery product (the roofline peak) and mad.lo alone (context)
+    # IMAD ceilings of this GPU (project microbenchmark): mad.lo alone (the
+    # roofline peak) and the lo/hi mix (context)
     sink = torch.empty(148 * 8 * 256 * 4, dtype=torch.int32, device=dev)
     iters = 4096
     peaks = {}
@@ -368,16 +368,24 @@ def measure_extra(gm, wl, dev, imad_peak):
     o2 = torch.empty(gm.G2P_WORDS, dtype=torch.int64, device=dev)
     gm.msm_device(pts2, sc2_d, group=2, out=o2)
     torch.cuda.synchronize()
+    gm.profile_enable(True)
     e0.record()
     reps = 3
     for _ in range(reps):
         gm.msm_device(pts2, sc2_d, group=2, out=o2)
     e1.record()
     torch.cuda.synchronize()
+    phases2 = gm.profile_collect()
+    gm.profile_enable(False)
     t2 = e0.elapsed_time(e1) / reps / 1e3
     ops2 = wl.msm_roofline_imad(n2, 2)
+    acc2 = {}
+    for name, v in phases2:
+        if name != "start":
+            acc2.setdefault(name, []).append(v)
     out["g2_msm_2^18"] = {"points_per_s": n2 / t2, "ms": t2 * 1e3, "imad_frac": ops2 / t2 / imad_peak,
-                          "window_bits": gm.default_window(2, n2, 5)}
+                          "window_bits": gm.default_window(2, n2, 5),
+                          "phases_ms": {k: statistics.mean(v) for k, v in acc2.items()}}
     del pts2, sc2_d
     out["batched_512"] = measure_batched(gm, wl, dev)
     out["serving"] = measure_serving(gm, wl, dev)

@@ -64,6 +64,7 @@ C_API = [
     "gm_bases_create", "gm_bases_destroy", "gm_bases_count", "gm_bases_precompute", "gm_msm_resident", "gm_batch_plan_create",
     "gm_batch_plan_run", "gm_batch_plan_destroy", "gm_batch_plan_bytes", "gm_batch_plan_classes",
     "gm_batch_run", "gm_batch_workspace_bytes", "gm_g1_sum_projective_host",
+    "gm_host_selftest",
 ]
 
 

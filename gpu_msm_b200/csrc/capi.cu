@@ -596,6 +596,98 @@ int gm_g2_sum_projective(gm_stream_t stream, uint32_t gpu_index, G2ProjectivePoi
   return e == cudaSuccess ? gm::GM_OK : gm::record_error(e, "k_proj_sum");
 }
 
+}  // extern "C"
+
+// Self-test of the host arithmetic used by the window combination.
+namespace {
+uint64_t st_next(uint64_t &s) {
+  s ^= s << 13;
+  s ^= s >> 7;
+  s ^= s << 17;
+  return s;
+}
+void st_fp(gm_host::HFp &a, uint64_t &s) {
+  for (int i = 0; i < 7; i++) a.v[i] = st_next(s);
+  a.v[6] &= 0x0fffffffffffffffULL;  // < 2^444 < p
+}
+template <class F>
+bool st_same_affine(const gm_host::HXyzz<F> &a, const uint64_t *proj) {
+  // XYZZ a against projective (X, Y, Z): X_a ZZZ_a Z == X ZZ_a ZZZ_a ... compare
+  // x = X_a / ZZ_a with X / Z and y = Y_a / ZZZ_a with Y / Z by cross products
+  typename F::T X, Y, Z, l, r;
+  memcpy(&X, proj, sizeof(X));
+  memcpy(&Y, proj + F::WORDS, sizeof(Y));
+  memcpy(&Z, proj + 2 * F::WORDS, sizeof(Z));
+  const bool inf_a = gm_host::hx_is_inf(a), inf_b = F::is_zero(Z);
+  if (inf_a || inf_b) return inf_a == inf_b;
+  F::mul(l, a.X, Z);
+  F::mul(r, X, a.ZZ);
+  if (memcmp(&l, &r, sizeof(l))) return false;
+  F::mul(l, a.Y, Z);
+  F::mul(r, Y, a.ZZZ);
+  return memcmp(&l, &r, sizeof(l)) == 0;
+}
+template <class F>
+int st_horner(uint64_t &seed, void (*fill)(typename F::T &, uint64_t &)) {
+  gm_host::HXyzz<F> sums[9];
+  for (int w = 0; w < 9; w++) {
+    fill(sums[w].X, seed);
+    fill(sums[w].Y, seed);
+    typename F::T z;
+    fill(z, seed);
+    F::sqr(sums[w].ZZ, z);
+    F::mul(sums[w].ZZZ, sums[w].ZZ, z);
+  }
+  memset(&sums[3], 0, sizeof(sums[3]));  // an empty window
+  uint64_t out[3 * 14];
+  gm_host::HXyzz<F> ref;
+  for (int c : {1, 5, 13}) {
+    gm_host::horner_to_proj<F>(out, sums, 9, c);
+    gm_host::horner_xyzz<F>(ref, sums, 9, c);
+    if (!st_same_affine<F>(ref, out)) return 1;
+  }
+  return 0;
+}
+void st_f1(gm_host::HFp &a, uint64_t &s) { st_fp(a, s); }
+void st_f2(gm_host::HFp2 &a, uint64_t &s) {
+  st_fp(a.c0, s);
+  st_fp(a.c1, s);
+}
+}  // namespace
+
+extern "C" {
+
+int gm_host_selftest(void) {
+  uint64_t seed = 0x9e3779b97f4a7c15ULL;
+  // squaring against the general product: edge values and random elements
+  gm_host::HFp a, x, y;
+  for (int k = 0; k < 2000; k++) {
+    if (k < 4) {
+      memset(&a, 0, sizeof(a));
+      if (k == 1) a.v[0] = 1;
+      if (k >= 2) {
+        memcpy(a.v, gm_host::P, sizeof(a.v));
+        a.v[0] -= (uint64_t)(k - 1);  // p - 1, p - 2
+      }
+    } else {
+      st_fp(a, seed);
+    }
+    gm_host::F1::sqr(x, a);
+    gm_host::F1::mul(y, a, a);
+    if (memcmp(&x, &y, sizeof(x))) return 1;
+  }
+  for (int k = 0; k < 500; k++) {
+    gm_host::HFp2 b, u, v;
+    st_f2(b, seed);
+    gm_host::F2::sqr(u, b);
+    gm_host::F2::mul(v, b, b);
+    if (memcmp(&u, &v, sizeof(u))) return 2;
+  }
+  if (st_horner<gm_host::F1>(seed, st_f1)) return 3;
+  if (st_horner<gm_host::F2>(seed, st_f2)) return 4;
+  return 0;
+}
+
 int gm_g1_sum_projective_host(G1ProjectivePoint *out, const G1ProjectivePoint *in, int n) {
   if (n < 0 || out == nullptr || (n > 0 && in == nullptr)) return gm::GM_ERR_ARG;
   gm_host::HXyzz<gm_host::F1> acc;

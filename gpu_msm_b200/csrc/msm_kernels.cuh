@@ -53,7 +53,7 @@ struct OutOfLine<Fp> {
 };
 template <>
 struct OutOfLine<Fp2> {
-  using type = Fp2Out;
+  using type = Fp2Call;
 };
 
 // Policy of the accumulation loop (one out-of-line product only).
@@ -63,9 +63,13 @@ template <>
 struct AccPolicy<Fp> {
   using type = FpOutMulOnly;
 };
+// G2: the whole Fp2 product out of line.  Inlined Karatsuba sums around 30
+// Fp calls made the loop overflow the instruction cache (ncu: 9.9% of warp
+// samples stalled on instruction fetch against 1.2% for G1); measured
+// 12.35 ms against 14.76 ms for the G2 2^18 accumulation.
 template <>
 struct AccPolicy<Fp2> {
-  using type = Fp2Out;
+  using type = Fp2Call;
 };
 
 template <class A, class B>
@@ -475,6 +479,37 @@ constexpr int acc_smem_bytes() {
   return 2 * (F::LIMBS / 2) * ACC_THREADS * 16;
 }
 
+// An affine base held in the accumulation kernel's shared-memory stage
+// ([chunk][thread] uint4 layout), read word by word at first use; y is
+// negated for a negative digit.
+template <class F, int CH>
+struct StagedPoint {
+  const uint4 (*rec)[ACC_THREADS];
+  int tid;
+  bool negate;
+  GM_DEVI typename F::T x() const {
+    typename F::T r;
+#pragma unroll
+    for (int k = 0; k < F::LIMBS; k++) {
+      const uint4 v = rec[k >> 2][tid];
+      const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+      limb_ref<F>(r, k) = w[k & 3];
+    }
+    return r;
+  }
+  GM_DEVI typename F::T y() const {
+    typename F::T r;
+#pragma unroll
+    for (int k = 0; k < F::LIMBS; k++) {
+      const int idx = F::LIMBS + k;
+      const uint4 v = rec[idx >> 2][tid];
+      const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+      limb_ref<F>(r, k) = w[idx & 3];
+    }
+    return negate ? F::neg(r) : r;
+  }
+};
+
 // The base of the next entry is staged into shared memory with cp.async while
 // the current mixed addition runs, so the random 112/224-byte gather is off
 // the critical path.  Each thread owns two slots (double buffer); slots are
@@ -529,22 +564,7 @@ __global__ void __launch_bounds__(ACC_THREADS) k_accumulate(const uint4 *__restr
       cp_async_commit();
       const uint32_t e_after = (pos + 2 < end) ? __ldg(entries + pos + 2) : 0u;
       cp_async_wait_prev();
-      T x, y;
-#pragma unroll
-      for (int q = 0; q < CH; q++) {
-        const uint4 v = stage[slot][q][tid];
-        const uint32_t w[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-        for (int e = 0; e < 4; e++) {
-          const int idx = 4 * q + e;
-          if (idx < F::LIMBS)
-            limb_ref<F>(x, idx) = w[e];
-          else
-            limb_ref<F>(y, idx - F::LIMBS) = w[e];
-        }
-      }
-      if (e_cur & 1u) y = F::neg(y);
-      xyzz_madd<FA>(acc, x, y);
+      xyzz_madd_pt<FA>(acc, StagedPoint<F, CH>{stage[slot], tid, (e_cur & 1u) != 0});
       pos++;
       slot ^= 1;
       e_cur = e_nxt;

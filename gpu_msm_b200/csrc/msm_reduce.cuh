@@ -48,8 +48,15 @@ __global__ void __launch_bounds__(128) k_red_level0(const xyzz_t<F> *__restrict_
     const int j0 = s * L0, j1 = min(B, j0 + L0);
     if (__ldg(offsets + kb + j0) != __ldg(offsets + kb + j1)) {  // any entries in the segment
       for (int j = j1 - 1; j >= j0; j--) {
-        if (__ldg(offsets + kb + j + 1) != __ldg(offsets + kb + j)) xyzz_add<FA>(acc, as_xyzz<FA>(buckets[kb + j]));
-        xyzz_add<FA>(ws, acc);
+        if constexpr (sizeof(typename F::T) == sizeof(fp_t)) {
+          if (__ldg(offsets + kb + j + 1) != __ldg(offsets + kb + j)) xyzz_add<FA>(acc, as_xyzz<FA>(buckets[kb + j]));
+          xyzz_add<FA>(ws, acc);
+        } else {
+          // Fp2: the addition out of line keeps the loop within the register file
+          if (__ldg(offsets + kb + j + 1) != __ldg(offsets + kb + j))
+            xyzz_add_cold<FA>(acc, as_xyzz<FA>(buckets[kb + j]));
+          xyzz_add_cold<FA>(ws, acc);
+        }
       }
     }
     X[g * M + s] = as_xyzz<F>(ws);
@@ -235,12 +242,14 @@ struct RedLayout {
   size_t o_X = 0, o_A0 = 0, o_t[2] = {0, 0};
 
   // wave_threads: level-0 threads resident at once on the device.  L0 is at
-  // least 16 buckets, and larger when G*B/16 segments would not fit one wave.
+  // least 16 buckets for G1 and 4 for G2 (an Fp2 addition takes three times
+  // as long, so G2 wants shorter chains), and larger when the segments would
+  // not fit one wave.
   template <class F, class Carver>
   void plan(int64_t G_, int B_, int64_t wave_threads, Carver &cv) {
     G = G_;
     B = B_;
-    int64_t l0 = 16;
+    int64_t l0 = sizeof(typename F::T) == sizeof(fp_t) ? 16 : 4;
     if (wave_threads > 0) l0 = std::max<int64_t>(l0, (G * B + wave_threads - 1) / wave_threads);
     L0 = (int)std::min<int64_t>(l0, B);
     nseg0 = (B + L0 - 1) / L0;

@@ -92,37 +92,51 @@ __device__ __noinline__ void xyzz_dbl_exc(xyzz_t<F> &p) {
   xyzz_dbl<F>(p, p);
 }
 
-// acc += (x2, y2) (madd-2008-s)
+// acc += (x2, y2) (madd-2008-s).  The products are ordered so that few
+// values are live at once (each value dies at its last use), which keeps
+// the Fp2 form within the register file.  The affine point comes from a
+// provider with x() and y(): registers (RegPoint), or a shared-memory stage
+// read at first use, so that the point is not held in registers across the
+// out-of-line products.
 template <class F>
-GM_DEVI void xyzz_madd(xyzz_t<F> &acc, const typename F::T &x2, const typename F::T &y2) {
+struct RegPoint {
+  const typename F::T &x_, &y_;
+  GM_DEVI const typename F::T &x() const { return x_; }
+  GM_DEVI const typename F::T &y() const { return y_; }
+};
+
+template <class F, class PT>
+GM_DEVI void xyzz_madd_pt(xyzz_t<F> &acc, const PT &pt) {
   using T = typename F::T;
   if (xyzz_is_inf(acc)) {
-    acc.X = x2;
-    acc.Y = y2;
+    acc.X = pt.x();
+    acc.Y = pt.y();
     acc.ZZ = F::one();
     acc.ZZZ = F::one();
     return;
   }
-  const T U2 = F::mul(x2, acc.ZZ);
-  const T S2 = F::mul(y2, acc.ZZZ);
-  const T P = F::sub(U2, acc.X);
-  const T R = F::sub(S2, acc.Y);
+  const T P = F::sub(F::mul(pt.x(), acc.ZZ), acc.X);    // U2 - X1
+  const T R = F::sub(F::mul(pt.y(), acc.ZZZ), acc.Y);   // S2 - Y1
   if (F::is_zero(P)) {
     if (F::is_zero(R))
-      xyzz_mdbl_cold<F>(acc, x2, y2);
+      xyzz_mdbl_cold<F>(acc, pt.x(), pt.y());
     else
       xyzz_set_inf(acc);
     return;
   }
   const T PP = F::sqr(P);
+  acc.ZZ = F::mul(acc.ZZ, PP);
   const T PPP = F::mul(P, PP);
+  acc.ZZZ = F::mul(acc.ZZZ, PPP);
   const T Q = F::mul(acc.X, PP);
   const T X3 = F::sub(F::sub(F::sqr(R), PPP), F::dbl(Q));
-  const T Y3 = F::sub(F::mul(R, F::sub(Q, X3)), F::mul(acc.Y, PPP));
-  acc.ZZ = F::mul(acc.ZZ, PP);
-  acc.ZZZ = F::mul(acc.ZZZ, PPP);
+  acc.Y = F::sub(F::mul(R, F::sub(Q, X3)), F::mul(acc.Y, PPP));
   acc.X = X3;
-  acc.Y = Y3;
+}
+
+template <class F>
+GM_DEVI void xyzz_madd(xyzz_t<F> &acc, const typename F::T &x2, const typename F::T &y2) {
+  xyzz_madd_pt<F>(acc, RegPoint<F>{x2, y2});
 }
 
 // acc += q (add-2008-s)

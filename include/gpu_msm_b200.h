@@ -240,6 +240,11 @@ int gm_g1_sum_projective(gm_stream_t stream, uint32_t gpu_index, G1ProjectivePoi
 int gm_g2_sum_projective(gm_stream_t stream, uint32_t gpu_index, G2ProjectivePoint *d_out,
                          const G2ProjectivePoint *d_in, int n);
 
+/* Self-test of the host arithmetic of the window combination (Montgomery
+ * squaring against the general product, Jacobian-doubling Horner against the
+ * XYZZ one); 0 when every check passes.  No reference counterpart. */
+int gm_host_selftest(void);
+
 /* Host-side sum of n G1 projective points (Montgomery form): combines the
  * partial results of a sharded MSM on a CPU; no reference counterpart. */
 int gm_g1_sum_projective_host(G1ProjectivePoint *out, const G1ProjectivePoint *in, int n);

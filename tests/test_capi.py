@@ -46,6 +46,12 @@ def test_library_exports_reference_cxx_api():
     assert not missing, missing
 
 
+def test_host_arithmetic_selftest():
+    """The host window combination's squaring and Jacobian doublings agree
+    with the general product and the XYZZ formulas."""
+    assert gm.lib().gm_host_selftest() == 0
+
+
 def test_struct_sizes():
     assert (gm.G1.itemsize, gm.G2.itemsize, gm.G1P.itemsize, gm.G2P.itemsize) == (120, 232, 168, 336)
 
