@@ -287,12 +287,12 @@ def run_ours(args, rank, world, local_rank):
                      "peak": imad_peak / 1e12, "unit": "TIMAD/s", "frac": achieved / imad_peak,
                      # dram__bytes_read + dram__bytes_write of one launch, from the ncu
                      # capture summarised in profiles/k_accumulate_g1_2p20.md
-                     "traffic": 1.656e9,
+                     "traffic": 1.592e9,
                      "traffic_unit": "bytes per launch (ncu)",
                      "work": f"798 IMAD x 10 Fp mults x {entries} entries per launch",
                      "peak_source": "measured: gm_imad_probe mode 1 (independent mad.lo chains over all SMs)",
                      "peak_lo_hi_mix": peaks[0] / 1e12,
-                     "imad_pipe_busy_ncu": 0.879},
+                     "imad_pipe_busy_ncu": 0.883},
         "msm_roofline": {"ops_imad": msm_ops, "achieved": msm_ops / (ms / 1e3) / 1e12,
                          "frac": msm_ops / (ms / 1e3) / imad_peak, "unit": "TIMAD/s"},
         "phases_ms": phase_ms,

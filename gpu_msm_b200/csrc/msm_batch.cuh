@@ -129,7 +129,7 @@ int batch_class_run(const BatchPlan &plan, const BatchClassPlan &cp, cudaStream_
   rc = reduce_launch<F>(s, cp.rl, buckets, offsets, ws, &src, &launches);
   if (rc) return rc;
   // precomputed mode: one window per MSM, so the combination is a conversion
-  k_combine_quad<F><<<grid_for(4 * (int64_t)cp.count, 128), 128, 0, s>>>(src, cp.count, cp.pc_stride ? 1 : cp.dp.W,
+  k_combine_quad<F><<<grid_for((int64_t)Coop<F>::LANES * cp.count, 128), 128, 0, s>>>(src, cp.count, cp.pc_stride ? 1 : cp.dp.W,
                                                                           cp.c, out_index, results);
   GM_CHECK_LAUNCH("k_combine_quad");
   launches++;

@@ -174,7 +174,7 @@ int reduce_launch(cudaStream_t s, const RedLayout &rl, const xyzz_t<F> *buckets,
   GM_CHECK_LAUNCH("k_red_level0");
   (*launches)++;
   if (rl.nseg1 > 0) {
-    k_red_level1<F><<<grid_for(4 * rl.G * rl.nseg1, 128), 128, 0, s>>>(A0, rl.G, rl.nseg0, rl.L1, rl.nseg1,
+    k_red_level1<F><<<grid_for((int64_t)Coop<F>::LANES * rl.G * rl.nseg1, 128), 128, 0, s>>>(A0, rl.G, rl.nseg0, rl.L1, rl.nseg1,
                                                                         rl.L0, X, rl.M);
     GM_CHECK_LAUNCH("k_red_level1");
     (*launches)++;
@@ -184,7 +184,7 @@ int reduce_launch(cudaStream_t s, const RedLayout &rl, const xyzz_t<F> *buckets,
   while (N > 1) {
     const int nout = (N + RedLayout::FAN - 1) / RedLayout::FAN;
     auto *dst = (xyzz_t<F> *)(ws + rl.o_t[k]);
-    k_tree_quad<F><<<grid_for(4 * rl.G * nout, 128), 128, 0, s>>>(src, rl.G, N, RedLayout::FAN, dst);
+    k_tree_quad<F><<<grid_for((int64_t)Coop<F>::LANES * rl.G * nout, 128), 128, 0, s>>>(src, rl.G, N, RedLayout::FAN, dst);
     GM_CHECK_LAUNCH("k_tree_quad");
     (*launches)++;
     src = dst;

@@ -8,12 +8,12 @@
 //     T_s = sum_r (r + 1) V_{s L0 + r},   A_s = sum_r V_{s L0 + r},
 // two additions per bucket and nothing else.  Then
 //     S_g = sum_s T_s + L0 * sum_s s A_s.
-// Level 1 cuts the A_s into segments of L1; a quad of lanes per segment s'
-// computes  D = sum_r r A_{s' L1 + r},  A' = sum_r A_{s' L1 + r}  and
+// Level 1 cuts the A_s into segments of L1; a cooperative group of lanes
+// (coop.cuh) per segment s' computes  D = sum_r r A_{s' L1 + r},  A' = sum_r A_{s' L1 + r}  and
 //     E_{s'} = L0 * (D + (s' L1) A')          (double-and-add, then doublings)
 // so that  sum_s s A_s = sum_{s'} (D + s' L1 A')  and
 //     S_g = sum_s T_s + sum_{s'} E_{s'}.
-// A quad-cooperative fan-in tree adds the nseg0 + nseg1 values of every group.
+// A cooperative fan-in tree adds the nseg0 + nseg1 values of every group.
 // Level 0 is throughput-bound (it holds nearly all the work and enough
 // threads to fill the GPU); the few, serial additions of level 1 and the tree
 // run on quads to cut their latency.  This replaces the reference's per-block
@@ -21,7 +21,7 @@
 // :2060-2179) with work that stays on the device.
 #pragma once
 #include "msm_kernels.cuh"
-#include "xyzz_quad.cuh"
+#include "coop.cuh"
 
 namespace gm {
 
@@ -64,13 +64,13 @@ __global__ void __launch_bounds__(128) k_red_level0(const xyzz_t<F> *__restrict_
   }
 }
 
-// Level 1: one quad per (group, segment s').  Writes E_{s'} to
-// X[g*M + nseg0 + s'].
+// Level 1: one cooperative group of lanes per (group, segment s').  Writes E_{s'} to X[g*M + nseg0 + s'].
 template <class F>
 __global__ void __launch_bounds__(128) k_red_level1(const xyzz_t<F> *__restrict__ A0, int64_t G, int nseg0, int L1,
                                                     int nseg1, int L0, xyzz_t<F> *__restrict__ X, int M) {
-  using FA = typename OutOfLine<F>::type;
-  const int64_t t = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 2;  // quad index
+  using C = Coop<F>;
+  using FA = typename C::A;
+  const int64_t t = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / C::LANES;
   if (t >= G * nseg1) return;
   const int64_t g = t / nseg1;
   const int s = (int)(t % nseg1);
@@ -79,31 +79,33 @@ __global__ void __launch_bounds__(128) k_red_level1(const xyzz_t<F> *__restrict_
   xyzz_set_inf(acc);
   xyzz_set_inf(ws);
   for (int r = r1 - 1; r >= r0; r--) {
-    q_add<FA>(acc, as_xyzz<FA>(A0[g * nseg0 + r]));
-    if (r > r0) q_add<FA>(ws, acc);
+    C::add(acc, as_xyzz<FA>(A0[g * nseg0 + r]));
+    if (r > r0) C::add(ws, acc);
   }
   // ws = sum (r - r0) A_r; add (s L1) * acc, then scale by L0
   xyzz_t<FA> m;
-  q_mul_small<FA>(m, acc, (uint32_t)r0);
-  q_add<FA>(ws, m);
-  q_mul_small<FA>(m, ws, (uint32_t)L0);
-  if (quad_lane() == 0) X[g * M + nseg0 + s] = as_xyzz<F>(m);
+  coop_mul_small<F>(m, acc, (uint32_t)r0);
+  C::add(ws, m);
+  coop_mul_small<F>(m, ws, (uint32_t)L0);
+  if (coop_leader<F>()) X[g * M + nseg0 + s] = as_xyzz<F>(m);
 }
 
-// out[g*nout + i] = sum_{k < fan} in[g*N + i*fan + k], one quad per output
+// out[g*nout + i] = sum_{k < fan} in[g*N + i*fan + k], one cooperative
+// group per output
 template <class F>
 __global__ void __launch_bounds__(128) k_tree_quad(const xyzz_t<F> *__restrict__ in, int64_t G, int N, int fan,
                                                    xyzz_t<F> *__restrict__ out) {
-  using FA = typename OutOfLine<F>::type;
+  using C = Coop<F>;
+  using FA = typename C::A;
   const int nout = (N + fan - 1) / fan;
-  const int64_t t = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 2;
+  const int64_t t = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / C::LANES;
   if (t >= G * nout) return;
   const int64_t g = t / nout;
   const int i = (int)(t % nout);
   const int64_t base = g * N + (int64_t)i * fan;
   xyzz_t<FA> acc = as_xyzz<FA>(in[base]);
-  for (int k = 1; k < fan && i * fan + k < N; k++) q_add<FA>(acc, as_xyzz<FA>(in[base + k]));
-  if (quad_lane() == 0) out[t] = as_xyzz<F>(acc);
+  for (int k = 1; k < fan && i * fan + k < N; k++) C::add(acc, as_xyzz<FA>(in[base + k]));
+  if (coop_leader<F>()) out[t] = as_xyzz<F>(acc);
 }
 
 // ---------------------------------------------------------------------------
@@ -112,7 +114,7 @@ __global__ void __launch_bounds__(128) k_tree_quad(const xyzz_t<F> *__restrict__
 // (part_head).  Runs of at most FIX_SHORT heads are folded serially by the
 // owner of the tail; longer runs (a bucket much larger than a slice, e.g. all
 // the scalars equal to 1) are queued and folded by k_fixup_long, one block of
-// 32 quads per run with a shared-memory tree.
+// cooperative groups per run with a shared-memory tree.
 // ---------------------------------------------------------------------------
 constexpr int FIX_SHORT = 8;
 constexpr int FIX_LONG_BLOCKS = 64;
@@ -162,9 +164,12 @@ __global__ void __launch_bounds__(128) k_fixup_long(const uint32_t *__restrict__
                                                     const xyzz_t<F> *__restrict__ part_tail,
                                                     const int32_t *__restrict__ head_key, uint32_t *__restrict__ err,
                                                     const int32_t *__restrict__ long_q, int64_t long_cap) {
-  using FA = typename OutOfLine<F>::type;
-  __shared__ xyzz_t<F> part[32];
-  const int quad = threadIdx.x >> 2;
+  using C = Coop<F>;
+  using FA = typename C::A;
+  constexpr int GROUPS = 128 / C::LANES;  // cooperative groups per block
+  __shared__ xyzz_t<F> part[GROUPS];
+  const int grp = threadIdx.x / C::LANES;
+  const bool leader = coop_leader<F>();
   const int64_t n_long = min((int64_t)long_q[0], long_cap);
   const uint32_t M = __ldg(offsets + K);
   const uint64_t chunk64 = ((uint64_t)M + nthreads - 1) / nthreads;
@@ -173,27 +178,25 @@ __global__ void __launch_bounds__(128) k_fixup_long(const uint32_t *__restrict__
     const int32_t k = long_q[1 + item];
     const int64_t t0 = (int64_t)(__ldg(offsets + k) / chunk);
     const int64_t t1 = min((int64_t)((__ldg(offsets + k + 1) - 1) / chunk), nthreads - 1);
-    // quad j folds run positions j, j+32, ... (position 0 is the tail piece)
+    // group j folds run positions j, j+GROUPS, ... (position 0 is the tail piece)
     xyzz_t<FA> acc;
     xyzz_set_inf(acc);
-    for (int64_t p = quad; p <= t1 - t0; p += 32) {
+    for (int64_t p = grp; p <= t1 - t0; p += GROUPS) {
       const int64_t ts = t0 + p;
       if (p == 0) {
-        q_add<FA>(acc, as_xyzz<FA>(part_tail[ts]));
+        C::add(acc, as_xyzz<FA>(part_tail[ts]));
       } else if (head_key[ts] != k) {
-        if (quad_lane() == 0) atomicOr(err, 1u);
+        if (leader) atomicOr(err, 1u);
       } else {
-        q_add<FA>(acc, as_xyzz<FA>(part_head[ts]));
+        C::add(acc, as_xyzz<FA>(part_head[ts]));
       }
     }
-    if (quad_lane() == 0) part[quad] = as_xyzz<F>(acc);
+    if (leader) part[grp] = as_xyzz<F>(acc);
     __syncthreads();
-    for (int h = 16; h >= 1; h >>= 1) {
-      if (quad < h) {
-        q_add<FA>(acc, as_xyzz<FA>(part[quad + h]));
-      }
+    for (int h = GROUPS / 2; h >= 1; h >>= 1) {
+      if (grp < h) C::add(acc, as_xyzz<FA>(part[grp + h]));
       __syncthreads();
-      if (quad < h && quad_lane() == 0) part[quad] = as_xyzz<F>(acc);
+      if (grp < h && leader) part[grp] = as_xyzz<F>(acc);
       __syncthreads();
     }
     if (threadIdx.x == 0) buckets[k] = part[0];
@@ -202,7 +205,7 @@ __global__ void __launch_bounds__(128) k_fixup_long(const uint32_t *__restrict__
 }
 
 // ---------------------------------------------------------------------------
-// Window combination on the device, one quad per MSM: result = sum_w
+// Window combination on the device, one cooperative group per MSM: result = sum_w
 // 2^(c w) S_w by Horner; homogeneous projective output (u64 limbs,
 // Montgomery).  out_index (optional) maps MSM i to its result slot.
 // ---------------------------------------------------------------------------
@@ -210,17 +213,18 @@ template <class F>
 __global__ void __launch_bounds__(128) k_combine_quad(const xyzz_t<F> *__restrict__ S, int n_msm, int W, int c,
                                                       const int32_t *__restrict__ out_index,
                                                       uint64_t *__restrict__ out_proj) {
-  using FA = typename OutOfLine<F>::type;
-  const int i = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 2);
+  using C = Coop<F>;
+  using FA = typename C::A;
+  const int i = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / C::LANES);
   if (i >= n_msm) return;
   xyzz_t<FA> res;
   xyzz_set_inf(res);
   for (int w = W - 1; w >= 0; w--) {
     if (!xyzz_is_inf(res))
-      for (int k = 0; k < c; k++) q_dbl<FA>(res);
-    q_add<FA>(res, as_xyzz<FA>(S[(int64_t)i * W + w]));
+      for (int k = 0; k < c; k++) C::dbl(res);
+    C::add(res, as_xyzz<FA>(S[(int64_t)i * W + w]));
   }
-  if (quad_lane() != 0) return;
+  if (!coop_leader<F>()) return;
   typename F::T Xp, Yp, Zp;
   xyzz_to_proj<FA>(Xp, Yp, Zp, res);
   constexpr int H = F::LIMBS / 2;
