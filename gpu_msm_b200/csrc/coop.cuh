@@ -23,7 +23,7 @@ struct Coop<Fp> {
 };
 template <>
 struct Coop<Fp2> {
-  using A = Fp2Out;
+  using A = Fp2Call;
   static constexpr int LANES = 4;
   GM_DEVI static void add(xyzz_t<A> &acc, const xyzz_t<A> &o) { q_add<A>(acc, o); }
   GM_DEVI static void dbl(xyzz_t<A> &p) { q_dbl<A>(p); }
