@@ -52,6 +52,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-extra", action="store_true", help="skip the Fp / G2 / CPU side measurements")
+    ap.add_argument("--msm-only", metavar="G,LOG2N", default=None,
+                    help="profiling workload: plain MSMs of group G (1 or 2) over 2^LOG2N synthetic points, "
+                         "--warmup untimed and --steps timed calls, one JSON line with time and phases")
     return ap.parse_args()
 
 
@@ -232,6 +235,42 @@ def run_reference(args, rank, world):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
+def run_msm_only(args):
+    """Plain single-GPU MSMs of one group and size (the workload the ncu
+    summaries of profiles/ are captured on for sizes other than the bench's)."""
+    import torch
+
+    import gpu_msm_b200 as gm
+    from gpu_msm_b200 import workload as wl
+    group, log2n = (int(x) for x in args.msm_only.split(","))
+    if group not in (1, 2) or not 1 <= log2n <= 24:
+        raise SystemExit("--msm-only G,LOG2N with G in {1, 2} and 1 <= LOG2N <= 24")
+    n = 1 << log2n
+    dev = torch.device("cuda", 0)
+    logs = wl.make_base_logs(n, seed=4343)
+    pts = gm.generator_mul_batch(torch.from_numpy(logs.view(np.int64)).to(dev), group=group)
+    sc = torch.from_numpy(wl.make_scalars(n, seed=43).view(np.int64)).to(dev)
+    out = torch.empty(gm.G1P_WORDS if group == 1 else gm.G2P_WORDS, dtype=torch.int64, device=dev)
+    for _ in range(args.warmup):
+        gm.msm_device(pts, sc, group=group, out=out)
+    torch.cuda.synchronize()
+    gm.profile_enable(True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        gm.msm_device(pts, sc, group=group, out=out)
+    e1.record()
+    torch.cuda.synchronize()
+    acc = {}
+    for k, v in gm.profile_collect():
+        if k != "start":
+            acc.setdefault(k, []).append(v)
+    gm.profile_enable(False)
+    ms = e0.elapsed_time(e1) / args.steps
+    print(json.dumps({"workload": f"plain G{group} MSM, n=2^{log2n}", "ms_per_msm": ms, "points_per_s": n / (ms / 1e3),
+                      "phases_ms": {k: statistics.mean(v) for k, v in acc.items()}}), flush=True)
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -623,6 +662,9 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.msm_only:
+        run_msm_only(args)
         return
     if world > 1:
         import datetime
