@@ -251,35 +251,65 @@ int host_msm(Prj *result, const Aff *points, const uint64_t *scalars, int limbs,
     proj_zero(result);
     return gm::GM_OK;
   }
-  cudaStream_t s;
+  // the scalars go first on s; the points follow on a second stream, so
+  // their copy overlaps the sort (which reads only the scalars)
+  cudaStream_t s, s2;
   if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return gm::GM_ERR_STREAM;
+  if (cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaStreamDestroy(s);
+    return gm::GM_ERR_STREAM;
+  }
+  cudaEvent_t alloc_done, pts_done;
+  if (cudaEventCreateWithFlags(&alloc_done, cudaEventDisableTiming) != cudaSuccess) {
+    cudaStreamDestroy(s);
+    cudaStreamDestroy(s2);
+    return gm::GM_ERR_STREAM;
+  }
+  if (cudaEventCreateWithFlags(&pts_done, cudaEventDisableTiming) != cudaSuccess) {
+    cudaEventDestroy(alloc_done);
+    cudaStreamDestroy(s);
+    cudaStreamDestroy(s2);
+    return gm::GM_ERR_STREAM;
+  }
   const size_t pts_bytes = (size_t)n * sizeof(Aff), sc_bytes = (size_t)n * limbs * sizeof(uint64_t);
   const size_t o_sc = (pts_bytes + 255) / 256 * 256;
   const size_t o_res = o_sc + (sc_bytes + 255) / 256 * 256;
   const size_t o_err = o_res + 512;
   char *buf = nullptr;
-  rc = gm::pool_alloc((int)gpu_index, s, o_err + 256, (void **)&buf);
-  if (rc) {
-    cudaStreamDestroy(s);
-    return rc;
-  }
   uint32_t err_host = 0;
-  cudaError_t e = cudaMemcpyAsync(buf, points, pts_bytes, cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(buf + o_sc, scalars, sc_bytes, cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess) {
-    rc = gm::msm_launch<F>(s, (int)gpu_index, nullptr, (const uint64_t *)buf, to_mont, (const uint64_t *)(buf + o_sc),
-                           limbs, n, (uint64_t *)(buf + o_res), 0, (uint32_t *)(buf + o_err));
-    if (rc == gm::GM_OK) {
-      e = cudaMemcpyAsync(result, buf + o_res, sizeof(Prj), cudaMemcpyDeviceToHost, s);
-      if (e == cudaSuccess) e = cudaMemcpyAsync(&err_host, buf + o_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+  cudaError_t e = cudaSuccess;
+  rc = gm::pool_alloc((int)gpu_index, s, o_err + 256, (void **)&buf);
+  if (rc == gm::GM_OK) {
+    e = cudaMemcpyAsync(buf + o_sc, scalars, sc_bytes, cudaMemcpyHostToDevice, s);
+    // the points' stream may use the buffer once its allocation is ordered
+    if (e == cudaSuccess) e = cudaEventRecord(alloc_done, s);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(s2, alloc_done, 0);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(buf, points, pts_bytes, cudaMemcpyHostToDevice, s2);
+    if (e == cudaSuccess) e = cudaEventRecord(pts_done, s2);
+    if (e == cudaSuccess) {
+      rc = gm::msm_launch<F>(s, (int)gpu_index, nullptr, (const uint64_t *)buf, to_mont,
+                             (const uint64_t *)(buf + o_sc), limbs, n, (uint64_t *)(buf + o_res), 0,
+                             (uint32_t *)(buf + o_err), pts_done);
+      if (rc == gm::GM_OK) {
+        e = cudaMemcpyAsync(result, buf + o_res, sizeof(Prj), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess)
+          e = cudaMemcpyAsync(&err_host, buf + o_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+      }
     }
+    // s waited for pts_done inside msm_launch, or waits here on an early error
+    cudaStreamWaitEvent(s, pts_done, 0);
+    cudaFreeAsync(buf, s);
   }
-  cudaFreeAsync(buf, s);
   cudaError_t se = cudaStreamSynchronize(s);
+  cudaError_t se2 = cudaStreamSynchronize(s2);
+  cudaEventDestroy(alloc_done);
+  cudaEventDestroy(pts_done);
   cudaStreamDestroy(s);
+  cudaStreamDestroy(s2);
   if (rc) return rc;
   if (e != cudaSuccess) return gm::record_error(e, "host_msm copy");
   if (se != cudaSuccess) return gm::record_error(se, "host_msm sync");
+  if (se2 != cudaSuccess) return gm::record_error(se2, "host_msm sync");
   if (err_host) return gm::GM_ERR_CHECK;
   return gm::GM_OK;
 }

@@ -15,9 +15,9 @@
 namespace gm {
 // heavy templates are instantiated once, in msm_g1.cu / msm_g2.cu
 extern template int msm_launch<Fp>(cudaStream_t, int, const uint4 *, const uint64_t *, int, const uint64_t *, int,
-                                   int64_t, uint64_t *, int, uint32_t *);
+                                   int64_t, uint64_t *, int, uint32_t *, cudaEvent_t);
 extern template int msm_launch<Fp2>(cudaStream_t, int, const uint4 *, const uint64_t *, int, const uint64_t *, int,
-                                    int64_t, uint64_t *, int, uint32_t *);
+                                    int64_t, uint64_t *, int, uint32_t *, cudaEvent_t);
 extern template int batch_layouts<Fp>(BatchPlan &, int);
 extern template int batch_layouts<Fp2>(BatchPlan &, int);
 extern template int batch_run<Fp>(const BatchPlan &, cudaStream_t, const uint64_t *, uint64_t *);

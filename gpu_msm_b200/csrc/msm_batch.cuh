@@ -107,15 +107,14 @@ int batch_class_run(const BatchPlan &plan, const BatchClassPlan &cp, cudaStream_
   GM_CHECK(cudaMemsetAsync(counts, 0, cp.K * sizeof(uint32_t), s));
   GM_CHECK(cudaMemsetAsync(err, 0, sizeof(uint32_t), s));
   GM_CHECK(cudaMemsetAsync(long_q, 0, sizeof(int32_t), s));
-  k_count_multi<<<grid_for(cp.P, 256), 256, 0, s>>>(scalars, plan.bases, Rec<F>::U4, F::LIMBS, cp.P, md, cp.dp,
-                                                    cp.pc_stride, counts);
+  k_count_multi<<<grid_for(cp.P, 256), 256, 0, s>>>(scalars, cp.P, md, cp.dp, cp.pc_stride, counts);
   GM_CHECK_LAUNCH("k_count_multi");
   k_scan_blocksum<<<(unsigned)cp.nb, SCAN_THREADS, 0, s>>>(counts, cp.K, bsum);
   k_scan_top<<<1, SCAN_THREADS, 0, s>>>(bsum, (int)cp.nb);
   k_scan_final<<<(unsigned)cp.nb, SCAN_THREADS, 0, s>>>(counts, cp.K, bsum, offsets);
   GM_CHECK_LAUNCH("k_scan");
-  k_scatter_multi<<<grid_for(cp.P, 256), 256, 0, s>>>(scalars, plan.bases, Rec<F>::U4, F::LIMBS, cp.P, md, cp.dp,
-                                                      cp.pc_stride, offsets, counts, entries);
+  k_scatter_multi<<<grid_for(cp.P, 256), 256, 0, s>>>(scalars, cp.P, md, cp.dp, cp.pc_stride, offsets, counts,
+                                                      entries);
   GM_CHECK_LAUNCH("k_scatter_multi");
   launches += 5;
   k_accumulate<F><<<grid_for(cp.nthreads, ACC_THREADS), ACC_THREADS, acc_smem_bytes<F>(), s>>>(

@@ -53,8 +53,11 @@ int default_window(int group, int64_t n, int limbs);
 // (reference-layout affine points; converted to Montgomery when to_mont) is
 // given.  Writes the projective result (reference layout) to out_proj.  When
 // err_out is non-null it receives the device consistency flag (0 = ok).
+// bases_ready (optional): an event the stream waits for after the sort,
+// before the bases are first read (the sort reads only the scalars).
 template <class F>
 int msm_launch(cudaStream_t s, int dev, const uint4 *bases, const uint64_t *ref_points, int to_mont,
-               const uint64_t *scalars, int limbs, int64_t n, uint64_t *out_proj, int c_override, uint32_t *err_out);
+               const uint64_t *scalars, int limbs, int64_t n, uint64_t *out_proj, int c_override, uint32_t *err_out,
+               cudaEvent_t bases_ready = nullptr);
 
 }  // namespace gm

@@ -197,10 +197,12 @@ int reduce_launch(cudaStream_t s, const RedLayout &rl, const xyzz_t<F> *buckets,
 
 // Runs the whole pipeline.  bases: packed records (or null to pack from
 // ref_points), scalars: device u64 limbs, out: reference projective layout.
+// bases_ready (optional): an event the stream waits for after the sort and
+// before it first reads the bases.
 template <class F>
 int msm_launch(cudaStream_t s, int dev, const uint4 *bases, const uint64_t *ref_points, int to_mont,
                const uint64_t *scalars, int limbs, int64_t n, uint64_t *out_proj, int c_override,
-               uint32_t *err_out) {
+               uint32_t *err_out, cudaEvent_t bases_ready) {
   constexpr int H = F::LIMBS / 2;  // u64 words per coordinate
   if (n == 0) {
     GM_CHECK(cudaMemsetAsync(out_proj, 0, 3 * H * sizeof(uint64_t), s));
@@ -242,6 +244,23 @@ int msm_launch(cudaStream_t s, int dev, const uint4 *bases, const uint64_t *ref_
   auto *err = (uint32_t *)(ws + lay.o_err);
   profile_mark(s, "start");
   int launches = 0;
+  // the sort needs only the scalars; the bases are packed after it, so a
+  // caller that is still copying them in can overlap that copy with the sort
+  GM_CHECK(cudaMemsetAsync(counts, 0, lay.K * sizeof(uint32_t), s));
+  GM_CHECK(cudaMemsetAsync(err, 0, sizeof(uint32_t), s));
+  auto *long_q = (int32_t *)(ws + lay.o_longq);
+  GM_CHECK(cudaMemsetAsync(long_q, 0, sizeof(int32_t), s));
+  k_count<<<grid_for(n, 256), 256, 0, s>>>(scalars, n, lay.dp, counts);
+  GM_CHECK_LAUNCH("k_count");
+  k_scan_blocksum<<<(unsigned)lay.nb, SCAN_THREADS, 0, s>>>(counts, lay.K, bsum);
+  k_scan_top<<<1, SCAN_THREADS, 0, s>>>(bsum, (int)lay.nb);
+  k_scan_final<<<(unsigned)lay.nb, SCAN_THREADS, 0, s>>>(counts, lay.K, bsum, offsets);
+  GM_CHECK_LAUNCH("k_scan");
+  k_scatter<<<grid_for(n, 256), 256, 0, s>>>(scalars, n, lay.dp, offsets, counts, entries);
+  GM_CHECK_LAUNCH("k_scatter");
+  launches += 5;
+  profile_mark(s, "sort");
+  if (bases_ready) GM_CHECK(cudaStreamWaitEvent(s, bases_ready, 0));
   if (bases == nullptr) {
     uint4 *packed = (uint4 *)(ws + lay.o_packed);
     k_pack_ref<F><<<grid_for(n, 256), 256, 0, s>>>(packed, ref_points, n, 2 * H + 1, to_mont);
@@ -250,21 +269,6 @@ int msm_launch(cudaStream_t s, int dev, const uint4 *bases, const uint64_t *ref_
     launches++;
     profile_mark(s, "pack");
   }
-  GM_CHECK(cudaMemsetAsync(counts, 0, lay.K * sizeof(uint32_t), s));
-  GM_CHECK(cudaMemsetAsync(err, 0, sizeof(uint32_t), s));
-  auto *long_q = (int32_t *)(ws + lay.o_longq);
-  GM_CHECK(cudaMemsetAsync(long_q, 0, sizeof(int32_t), s));
-  k_count<<<grid_for(n, 256), 256, 0, s>>>(scalars, bases, Rec<F>::U4, F::LIMBS, n, lay.dp, counts);
-  GM_CHECK_LAUNCH("k_count");
-  k_scan_blocksum<<<(unsigned)lay.nb, SCAN_THREADS, 0, s>>>(counts, lay.K, bsum);
-  k_scan_top<<<1, SCAN_THREADS, 0, s>>>(bsum, (int)lay.nb);
-  k_scan_final<<<(unsigned)lay.nb, SCAN_THREADS, 0, s>>>(counts, lay.K, bsum, offsets);
-  GM_CHECK_LAUNCH("k_scan");
-  k_scatter<<<grid_for(n, 256), 256, 0, s>>>(scalars, bases, Rec<F>::U4, F::LIMBS, n, lay.dp, offsets, counts,
-                                             entries);
-  GM_CHECK_LAUNCH("k_scatter");
-  launches += 5;
-  profile_mark(s, "sort");
   k_accumulate<F><<<grid_for(lay.nthreads, ACC_THREADS), ACC_THREADS, acc_smem_bytes<F>(), s>>>(bases, entries, offsets, lay.K, lay.nthreads, buckets,
                                                                head, tail, hk, tk);
   GM_CHECK_LAUNCH("k_accumulate");

@@ -276,11 +276,12 @@ GM_DEVI void for_each_digit(const uint64_t *__restrict__ scalar, const DigitPara
   }
 }
 
-static __global__ void k_count(const uint64_t *__restrict__ scalars, const uint4 *__restrict__ bases, int rec_u4,
-                        int field_limbs, int64_t n, DigitParams dp, uint32_t *__restrict__ counts) {
+// The sort reads only the scalars: entries of bases at infinity are sorted
+// like any other and skipped by the accumulation.
+static __global__ void k_count(const uint64_t *__restrict__ scalars, int64_t n, DigitParams dp,
+                               uint32_t *__restrict__ counts) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  if (base_is_inf(bases + i * rec_u4, rec_u4, field_limbs)) return;
   for_each_digit(scalars + i * dp.limbs, dp, [&](int w, int d) {
     const int b = (d < 0 ? -d : d) - 1;
     atomicAdd(&counts[w * dp.B + b], 1u);
@@ -288,12 +289,11 @@ static __global__ void k_count(const uint64_t *__restrict__ scalars, const uint4
 }
 
 // Consumes counts back down to zero; entry = (point index << 1) | negative.
-static __global__ void k_scatter(const uint64_t *__restrict__ scalars, const uint4 *__restrict__ bases, int rec_u4,
-                          int field_limbs, int64_t n, DigitParams dp, const uint32_t *__restrict__ offsets,
-                          uint32_t *__restrict__ counts, uint32_t *__restrict__ entries) {
+static __global__ void k_scatter(const uint64_t *__restrict__ scalars, int64_t n, DigitParams dp,
+                                 const uint32_t *__restrict__ offsets, uint32_t *__restrict__ counts,
+                                 uint32_t *__restrict__ entries) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  if (base_is_inf(bases + i * rec_u4, rec_u4, field_limbs)) return;
   for_each_digit(scalars + i * dp.limbs, dp, [&](int w, int d) {
     const int key = w * dp.B + (d < 0 ? -d : d) - 1;
     const uint32_t rank = atomicSub(&counts[key], 1u) - 1u;
@@ -328,31 +328,27 @@ GM_DEVI int msm_of(const int64_t *__restrict__ ps, int count, int64_t p) {
   return lo;
 }
 
-static __global__ void k_count_multi(const uint64_t *__restrict__ scalars, const uint4 *__restrict__ bases,
-                                     int rec_u4, int field_limbs, int64_t P, MultiDesc md, DigitParams dp,
+static __global__ void k_count_multi(const uint64_t *__restrict__ scalars, int64_t P, MultiDesc md, DigitParams dp,
                                      int64_t pc_stride, uint32_t *__restrict__ counts) {
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P) return;
   const int i = msm_of(md.point_start, md.count, p);
   const int64_t j = p - __ldg(md.point_start + i);
   const int64_t bi = __ldg(md.base_off + i) + j;
-  if (base_is_inf(bases + bi * rec_u4, rec_u4, field_limbs)) return;
   const int64_t kbase = (int64_t)i * (pc_stride ? 1 : dp.W) * dp.B;
   for_each_digit(scalars + (__ldg(md.sc_off + i) + j) * dp.limbs, dp, [&](int w, int d) {
     atomicAdd(&counts[kbase + (pc_stride ? 0 : (int64_t)w * dp.B) + (d < 0 ? -d : d) - 1], 1u);
   });
 }
 
-static __global__ void k_scatter_multi(const uint64_t *__restrict__ scalars, const uint4 *__restrict__ bases,
-                                       int rec_u4, int field_limbs, int64_t P, MultiDesc md, DigitParams dp,
-                                       int64_t pc_stride, const uint32_t *__restrict__ offsets,
+static __global__ void k_scatter_multi(const uint64_t *__restrict__ scalars, int64_t P, MultiDesc md,
+                                       DigitParams dp, int64_t pc_stride, const uint32_t *__restrict__ offsets,
                                        uint32_t *__restrict__ counts, uint32_t *__restrict__ entries) {
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P) return;
   const int i = msm_of(md.point_start, md.count, p);
   const int64_t j = p - __ldg(md.point_start + i);
   const int64_t bi = __ldg(md.base_off + i) + j;
-  if (base_is_inf(bases + bi * rec_u4, rec_u4, field_limbs)) return;
   const int64_t kbase = (int64_t)i * (pc_stride ? 1 : dp.W) * dp.B;
   for_each_digit(scalars + (__ldg(md.sc_off + i) + j) * dp.limbs, dp, [&](int w, int d) {
     const int64_t key = kbase + (pc_stride ? 0 : (int64_t)w * dp.B) + (d < 0 ? -d : d) - 1;
@@ -497,6 +493,17 @@ struct StagedPoint {
     }
     return r;
   }
+  // packed records of the point at infinity hold x = y = 0, which is not a
+  // curve point (b != 0)
+  GM_DEVI bool is_inf() const {
+    uint32_t o = 0;
+#pragma unroll
+    for (int q = 0; q < F::LIMBS / 2; q++) {
+      const uint4 v = rec[q][tid];
+      o |= v.x | v.y | v.z | v.w;
+    }
+    return o == 0;
+  }
   GM_DEVI typename F::T y() const {
     typename F::T r;
 #pragma unroll
@@ -564,7 +571,10 @@ __global__ void __launch_bounds__(ACC_THREADS) k_accumulate(const uint4 *__restr
       cp_async_commit();
       const uint32_t e_after = (pos + 2 < end) ? __ldg(entries + pos + 2) : 0u;
       cp_async_wait_prev();
-      xyzz_madd_pt<FA>(acc, StagedPoint<F, CH>{stage[slot], tid, (e_cur & 1u) != 0});
+      {
+        const StagedPoint<F, CH> pt{stage[slot], tid, (e_cur & 1u) != 0};
+        if (!pt.is_inf()) xyzz_madd_pt<FA>(acc, pt);
+      }
       pos++;
       slot ^= 1;
       e_cur = e_nxt;

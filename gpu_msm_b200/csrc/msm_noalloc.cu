@@ -121,14 +121,13 @@ extern "C" int gm_g1_msm_device_noalloc(gm_stream_t stream, uint32_t gpu_index, 
   GM_CHECK(cudaMemsetAsync(err, 0, sizeof(uint32_t), s));
   gm::k_pack_ref<Fp><<<grid_of(n, 256), 256, 0, s>>>(packed, (const uint64_t *)d_points, n, 2 * H + 1, 0);
   GM_CHECK_LAUNCH("k_pack_ref");
-  gm::k_count<<<grid_of(n, 256), 256, 0, s>>>(d_scalars, packed, gm::Rec<Fp>::U4, Fp::LIMBS, n, lay.dp, counts);
+  gm::k_count<<<grid_of(n, 256), 256, 0, s>>>(d_scalars, n, lay.dp, counts);
   GM_CHECK_LAUNCH("k_count");
   gm::k_scan_blocksum<<<(unsigned)lay.nb, gm::SCAN_THREADS, 0, s>>>(counts, lay.K, bsum);
   gm::k_scan_top<<<1, gm::SCAN_THREADS, 0, s>>>(bsum, (int)lay.nb);
   gm::k_scan_final<<<(unsigned)lay.nb, gm::SCAN_THREADS, 0, s>>>(counts, lay.K, bsum, offsets);
   GM_CHECK_LAUNCH("k_scan");
-  gm::k_scatter<<<grid_of(n, 256), 256, 0, s>>>(d_scalars, packed, gm::Rec<Fp>::U4, Fp::LIMBS, n, lay.dp, offsets,
-                                                 counts, entries);
+  gm::k_scatter<<<grid_of(n, 256), 256, 0, s>>>(d_scalars, n, lay.dp, offsets, counts, entries);
   GM_CHECK_LAUNCH("k_scatter");
   gm::k_accumulate<Fp><<<grid_of(lay.nthreads, gm::ACC_THREADS), gm::ACC_THREADS, gm::acc_smem_bytes<Fp>(), s>>>(
       packed, entries, offsets, lay.K, lay.nthreads, buckets, head, tail, hk, tk);
