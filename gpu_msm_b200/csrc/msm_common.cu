@@ -152,14 +152,39 @@ int64_t launches_and_reset() {
 constexpr size_t TAIL_SLOT_BYTES = PINNED_SLOT_BYTES;  // >= 257 windows x 448 B + 336 B
 static std::mutex g_pin_mu;
 static std::vector<void *> g_pin_free;
+// Slots whose last copy is still pending: returned to the free list once
+// their event has completed.  A host function per release would cost a
+// driver round trip (~0.2 ms of stream time on B200 boxes) for nothing.
+struct PendingSlot {
+  void *slot;
+  cudaEvent_t ev;
+  int dev;
+};
+static std::vector<PendingSlot> g_pin_pending;
+static std::map<int, std::vector<cudaEvent_t>> g_free_events;  // per device
 static bool g_host_tail = true;
 
 bool host_tail_enabled() { return g_host_tail; }
 void set_host_tail_enabled(bool on) { g_host_tail = on; }
 
+// caller holds g_pin_mu
+static void reclaim_completed_slots() {
+  for (size_t i = 0; i < g_pin_pending.size();) {
+    if (cudaEventQuery(g_pin_pending[i].ev) == cudaSuccess) {
+      g_pin_free.push_back(g_pin_pending[i].slot);
+      g_free_events[g_pin_pending[i].dev].push_back(g_pin_pending[i].ev);
+      g_pin_pending[i] = g_pin_pending.back();
+      g_pin_pending.pop_back();
+    } else {
+      i++;
+    }
+  }
+}
+
 int pinned_acquire(void **p) {
   {
     std::lock_guard<std::mutex> lk(g_pin_mu);
+    if (g_pin_free.empty()) reclaim_completed_slots();
     if (!g_pin_free.empty()) {
       *p = g_pin_free.back();
       g_pin_free.pop_back();
@@ -176,11 +201,39 @@ void pinned_release(void *p) {
   g_pin_free.push_back(p);
 }
 
+// The slot returns to the pool once the work enqueued on s so far has run.
+int enqueue_pinned_release(cudaStream_t s, void *slot) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return record_error(e, "cudaGetDevice");
+  cudaEvent_t ev = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    auto &fe = g_free_events[dev];
+    if (!fe.empty()) {
+      ev = fe.back();
+      fe.pop_back();
+    }
+  }
+  if (ev == nullptr) {
+    e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    // without an event the slot stays with the stream's pending work: leak it
+    // rather than hand it out again while a copy may still use it
+    if (e != cudaSuccess) return record_error(e, "cudaEventCreate(slot)");
+  }
+  e = cudaEventRecord(ev, s);
+  if (e != cudaSuccess) return record_error(e, "cudaEventRecord(slot)");
+  std::lock_guard<std::mutex> lk(g_pin_mu);
+  g_pin_pending.push_back(PendingSlot{slot, ev, dev});
+  return GM_OK;
+}
+
 struct TailCtx {
   int group, W, c;
   char *slot;
 };
 
+// Horner over the window sums in the slot; the result goes after them.
 static void CUDART_CB tail_compute(void *p) {
   auto *t = static_cast<TailCtx *>(p);
   if (t->group == 1) {
@@ -192,18 +245,6 @@ static void CUDART_CB tail_compute(void *p) {
     gm_host::horner_to_proj<gm_host::F2>(out, reinterpret_cast<const gm_host::HXyzz<gm_host::F2> *>(t->slot), t->W,
                                          t->c);
   }
-}
-
-static void CUDART_CB slot_release(void *p) { pinned_release(p); }
-
-int enqueue_pinned_release(cudaStream_t s, void *slot) {
-  cudaError_t e = cudaLaunchHostFunc(s, slot_release, slot);
-  return e == cudaSuccess ? GM_OK : record_error(e, "cudaLaunchHostFunc(release)");
-}
-
-static void CUDART_CB tail_release(void *p) {
-  auto *t = static_cast<TailCtx *>(p);
-  pinned_release(t->slot);
   delete t;
 }
 
@@ -225,15 +266,16 @@ int enqueue_host_tail(cudaStream_t s, int group, const void *d_sums, int W, int 
     return record_error(e, "tail D2H");
   }
   e = cudaLaunchHostFunc(s, tail_compute, t);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(d_out, static_cast<char *>(slot) + (size_t)W * elem, out_bytes, cudaMemcpyHostToDevice, s);
-  cudaError_t e2 = cudaLaunchHostFunc(s, tail_release, t);
-  if (e2 != cudaSuccess) {
-    // the slot stays with the stream's pending work; leak it rather than
-    // hand it out again while a copy may still read it
-    return record_error(e2, "tail release");
+  if (e != cudaSuccess) {
+    delete t;
+    // the D2H may still write the slot: release it in stream order
+    enqueue_pinned_release(s, slot);
+    return record_error(e, "tail host function");
   }
-  return e == cudaSuccess ? GM_OK : record_error(e, "tail host function");
+  e = cudaMemcpyAsync(d_out, static_cast<char *>(slot) + (size_t)W * elem, out_bytes, cudaMemcpyHostToDevice, s);
+  rc = enqueue_pinned_release(s, slot);
+  if (e != cudaSuccess) return record_error(e, "tail H2D");
+  return rc;
 }
 
 int device_sm_count(int dev, int *sms) {
