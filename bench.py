@@ -42,8 +42,8 @@ METRIC = "MSM points/s (G1 2^20, G2 2^18) batched vs plain on 1 B200, bit-exact;
 
 
 # fixed-base window tables (window widths) for the resident-table workloads
-PRECOMPUTE_BATCH = (8, 10, 12, 14)
-PRECOMPUTE_SERVE = {1: (11, 20), 2: (11, 16)}
+PRECOMPUTE_BATCH = (8, 10, 12, 14, 16)
+PRECOMPUTE_SERVE = {1: (11, 14, 17, 20), 2: (11, 13, 16)}
 
 def parse():
     ap = argparse.ArgumentParser()
