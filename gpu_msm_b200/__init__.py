@@ -64,7 +64,7 @@ C_API = [
     "gm_bases_create", "gm_bases_destroy", "gm_bases_count", "gm_bases_precompute", "gm_msm_resident", "gm_batch_plan_create",
     "gm_batch_plan_run", "gm_batch_plan_destroy", "gm_batch_plan_bytes", "gm_batch_plan_classes",
     "gm_batch_run", "gm_batch_workspace_bytes", "gm_g1_sum_projective_host",
-    "gm_host_selftest",
+    "gm_host_selftest", "gm_fp_elem", "gm_fp2_elem", "gm_g1_point_elem", "gm_g2_point_elem",
 ]
 
 
@@ -129,6 +129,10 @@ def lib() -> ctypes.CDLL:
         L.gm_batch_workspace_bytes.restype = i64
         for name in ("gm_g1_sum_projective", "gm_g2_sum_projective"):
             getattr(L, name).argtypes = [vp, u32, vp, vp, i32]
+        for name in ("gm_fp_elem", "gm_fp2_elem"):
+            getattr(L, name).argtypes = [vp, u32, i32, vp, vp, vp, ctypes.c_uint64, vp]
+        for name in ("gm_g1_point_elem", "gm_g2_point_elem"):
+            getattr(L, name).argtypes = [vp, u32, i32, vp, vp, vp, vp, i32, ctypes.c_uint64]
         _lib = L
     return _lib
 
@@ -424,6 +428,77 @@ def field_sqr_array(a, out=None, stream=None):
     _require(out, 7, "out", rows=a.shape[0])
     _check(lib().gm_fp_mont_sqr_array(_stream_handle(stream), _dev_index(a), ctypes.c_void_p(out.data_ptr()),
                                       ctypes.c_void_p(a.data_ptr()), a.shape[0]), "fp_mont_sqr")
+    return out
+
+
+# Single-element operations (gm_fp_elem, gm_fp2_elem, gm_g{1,2}_point_elem):
+# op names in the order of GM_FP_*, GM_FP2_* and GM_PT_* of
+# include/gpu_msm_b200.h.  They back the reference's stream APIs
+# fp_*_async / fp2_*_async / point_*_async (include/fp.h:158-204,
+# include/fp2.h:99-133, include/curve.h:156-211).
+FP_OPS = ("add", "sub", "mul", "neg", "inv", "div", "copy", "zero", "one", "to_mont", "from_mont", "mont_mul",
+          "cmp", "is_zero", "is_one", "cmov", "sqrt", "is_qr", "pow_u64")
+FP2_OPS = ("add", "sub", "mul", "square", "neg", "conjugate", "inv", "div", "copy", "mul_by_i", "frobenius",
+           "cmp", "is_zero", "is_one", "cmov", "mont_mul")
+POINT_OPS = ("add", "double", "neg", "scalar_mul", "scalar_mul_u64", "to_mont", "from_mont", "at_infinity")
+
+
+def _ptr_or_null(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else ctypes.c_void_p(0)
+
+
+def field_elem(op: str, a=None, b=None, c=None, arg: int = 0, fp2: bool = False, flag=None, stream=None):
+    """One Fp (or Fp2) element operation on int64 device tensors of shape
+    (1, 7) [(1, 14) for Fp2], asynchronous on the current torch stream.
+    ``c`` receives the result (allocated when None; read too by cmov);
+    ``flag`` (an int32 device tensor of one element, allocated when None)
+    receives cmp / is_zero / is_one / is_qr / sqrt's answer.  mul, inv, div,
+    square, sqrt, is_qr and pow_u64 work on standard-form values.
+    Returns (c, flag)."""
+    import torch
+    ops = FP2_OPS if fp2 else FP_OPS
+    code = ops.index(op)
+    cols = 14 if fp2 else 7
+    ref = a if a is not None else c
+    for t, what in ((a, "a"), (b, "b"), (c, "c")):
+        if t is not None:
+            _require(t, cols, what, rows=1)
+    dev = ref.device if ref is not None else torch.device("cuda", torch.cuda.current_device())
+    if c is None:
+        c = torch.zeros((1, cols), dtype=torch.int64, device=dev)
+    if flag is None:
+        flag = torch.zeros(1, dtype=torch.int32, device=dev)
+    fn = lib().gm_fp2_elem if fp2 else lib().gm_fp_elem
+    _check(fn(_stream_handle(stream), _dev_index(c), code, _ptr_or_null(c), _ptr_or_null(a), _ptr_or_null(b),
+              ctypes.c_uint64(arg & 0xFFFFFFFFFFFFFFFF), ctypes.c_void_p(flag.data_ptr())),
+           ("fp2_" if fp2 else "fp_") + op)
+    return c, flag
+
+
+def point_elem(op: str, p=None, q=None, scalar=None, scalar_u64: int = 0, group: int = 1, out=None, stream=None):
+    """One affine point operation (gm_g{1,2}_point_elem) on int64 device
+    tensors of shape (1, 15) [G1Point] or (1, 29) [G2Point], Montgomery form;
+    ``scalar`` is an int64 device tensor (1, limbs) for scalar_mul.  Returns
+    the result tensor."""
+    import torch
+    code = POINT_OPS.index(op)
+    cols = G1_WORDS if group == 1 else G2_WORDS
+    for t, what in ((p, "p"), (q, "q")):
+        if t is not None:
+            _require(t, cols, what, rows=1)
+    limbs = 0
+    if scalar is not None:
+        _require(scalar, None, "scalar", rows=1)
+        limbs = scalar.shape[1]
+    ref = p if p is not None else out
+    dev = ref.device if ref is not None else torch.device("cuda", torch.cuda.current_device())
+    if out is None:
+        out = torch.zeros((1, cols), dtype=torch.int64, device=dev)
+    _require(out, cols, "out", rows=1)
+    fn = lib().gm_g1_point_elem if group == 1 else lib().gm_g2_point_elem
+    _check(fn(_stream_handle(stream), _dev_index(out), code, ctypes.c_void_p(out.data_ptr()), _ptr_or_null(p),
+              _ptr_or_null(q), _ptr_or_null(scalar), limbs, ctypes.c_uint64(scalar_u64 & 0xFFFFFFFFFFFFFFFF)),
+           f"g{group}_point_{op}")
     return out
 
 

@@ -245,6 +245,89 @@ int gm_g2_sum_projective(gm_stream_t stream, uint32_t gpu_index, G2ProjectivePoi
  * XYZZ one); 0 when every check passes.  No reference counterpart. */
 int gm_host_selftest(void);
 
+/* Single-element operations on device pointers, asynchronous on `stream`:
+ * the C-ABI behind the reference's stream APIs fp_*_async
+ * (include/fp.h:158-204), fp2_*_async (include/fp2.h:99-133) and
+ * point_*_async<G1Point|G2Point> (include/curve.h:156-211), and behind its
+ * host-pointer helpers (include/fp_kernels.h:26-38, include/fp2_kernels.h:21-37).
+ *
+ * gm_fp_elem / gm_fp2_elem: c = op(a, b).  MUL, INV, DIV, SQUARE, SQRT, IS_QR
+ *   and POW_U64 work on standard-form values (the reference's fp_mul,
+ *   fp_inv, ... convert to and from Montgomery form inside); MONT_MUL is the
+ *   Montgomery product; inverses and quotients of 0 are 0.  CMOV: c = a when
+ *   (arg & 1), else c is left as it is.  POW_U64: c = a^arg.  CMP writes
+ *   -1 / 0 / 1 (limb-wise comparison, c0 before c1 for Fp2) to *d_flag;
+ *   IS_ZERO, IS_ONE and IS_QR write 0 / 1 there; SQRT writes c and 0 / 1
+ *   (a^((p+1)/4) for a quadratic residue, else c = 0 and 0).
+ * gm_g{1,2}_point_elem: affine points in Montgomery form.  ADD, DOUBLE, NEG
+ *   follow the reference's affine formulas and branch order
+ *   (src/curve.cu:72-227); SCALAR_MUL takes scalar_limbs little-endian u64
+ *   limbs at d_scalar, SCALAR_MUL_U64 the value scalar_u64; TO_MONT /
+ *   FROM_MONT convert both coordinates (infinity -> zeros + flag);
+ *   AT_INFINITY writes the identity.
+ * Inputs are canonical field elements (below p).  Returns -1 for an unknown
+ * op or a missing pointer the op needs. */
+enum {
+  GM_FP_ADD = 0,
+  GM_FP_SUB = 1,
+  GM_FP_MUL = 2,
+  GM_FP_NEG = 3,
+  GM_FP_INV = 4,
+  GM_FP_DIV = 5,
+  GM_FP_COPY = 6,
+  GM_FP_ZERO = 7,
+  GM_FP_ONE = 8,
+  GM_FP_TO_MONT = 9,
+  GM_FP_FROM_MONT = 10,
+  GM_FP_MONT_MUL = 11,
+  GM_FP_CMP = 12,
+  GM_FP_IS_ZERO = 13,
+  GM_FP_IS_ONE = 14,
+  GM_FP_CMOV = 15,
+  GM_FP_SQRT = 16,
+  GM_FP_IS_QR = 17,
+  GM_FP_POW_U64 = 18,
+  GM_FP_OP_COUNT = 19
+};
+enum {
+  GM_FP2_ADD = 0,
+  GM_FP2_SUB = 1,
+  GM_FP2_MUL = 2,
+  GM_FP2_SQUARE = 3,
+  GM_FP2_NEG = 4,
+  GM_FP2_CONJUGATE = 5,
+  GM_FP2_INV = 6,
+  GM_FP2_DIV = 7,
+  GM_FP2_COPY = 8,
+  GM_FP2_MUL_BY_I = 9,
+  GM_FP2_FROBENIUS = 10,
+  GM_FP2_CMP = 11,
+  GM_FP2_IS_ZERO = 12,
+  GM_FP2_IS_ONE = 13,
+  GM_FP2_CMOV = 14,
+  GM_FP2_MONT_MUL = 15,
+  GM_FP2_OP_COUNT = 16
+};
+enum {
+  GM_PT_ADD = 0,
+  GM_PT_DOUBLE = 1,
+  GM_PT_NEG = 2,
+  GM_PT_SCALAR_MUL = 3,
+  GM_PT_SCALAR_MUL_U64 = 4,
+  GM_PT_TO_MONT = 5,
+  GM_PT_FROM_MONT = 6,
+  GM_PT_AT_INFINITY = 7,
+  GM_PT_OP_COUNT = 8
+};
+int gm_fp_elem(gm_stream_t stream, uint32_t gpu_index, int op, Fp *d_c, const Fp *d_a, const Fp *d_b, uint64_t arg,
+               int32_t *d_flag);
+int gm_fp2_elem(gm_stream_t stream, uint32_t gpu_index, int op, Fp2 *d_c, const Fp2 *d_a, const Fp2 *d_b,
+                uint64_t arg, int32_t *d_flag);
+int gm_g1_point_elem(gm_stream_t stream, uint32_t gpu_index, int op, G1Point *d_r, const G1Point *d_p,
+                     const G1Point *d_q, const uint64_t *d_scalar, int scalar_limbs, uint64_t scalar_u64);
+int gm_g2_point_elem(gm_stream_t stream, uint32_t gpu_index, int op, G2Point *d_r, const G2Point *d_p,
+                     const G2Point *d_q, const uint64_t *d_scalar, int scalar_limbs, uint64_t scalar_u64);
+
 /* Host-side sum of n G1 projective points (Montgomery form): combines the
  * partial results of a sharded MSM on a CPU; no reference counterpart. */
 int gm_g1_sum_projective_host(G1ProjectivePoint *out, const G1ProjectivePoint *in, int n);

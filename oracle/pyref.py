@@ -149,3 +149,158 @@ def on_curve(p, group=1) -> bool:
     x, y = p
     b = B_G1 if group == 1 else B_G2
     return F.mul(y, y) == F.add(F.mul(F.mul(x, x), x), b)
+
+
+# ---- single-element operations (the reference's stream APIs) ----------------
+# Standard-form ints in, (result, flag) out, with the conventions of
+# src/fp.cu (fp_add ... fp_sqrt), src/fp2.cu and src/curve.cu:72-268.
+
+R_INV = pow(R_MONT, -1, P)
+
+
+def _inv0(v):
+    return pow(v, P - 2, P)  # Fermat: 0 -> 0 like fp_inv (src/fp.cu:522)
+
+
+def fp_elem(op, a=0, b=0, c=0, arg=0):
+    """One Fp operation; mul/inv/div/sqrt/is_qr/pow_u64 on standard form."""
+    if op == "add":
+        return (a + b) % P, 0
+    if op == "sub":
+        return (a - b) % P, 0
+    if op == "mul":
+        return a * b % P, 0
+    if op == "neg":
+        return (-a) % P, 0
+    if op == "inv":
+        return _inv0(a), 0
+    if op == "div":  # src/fp.cu:571: b == 0 -> 0
+        return (a * _inv0(b) % P if b else 0), 0
+    if op == "copy":
+        return a, 0
+    if op == "zero":
+        return 0, 0
+    if op == "one":
+        return 1, 0
+    if op == "to_mont":
+        return a * R_MONT % P, 0
+    if op == "from_mont":
+        return a * R_INV % P, 0
+    if op == "mont_mul":
+        return a * b * R_INV % P, 0
+    if op == "cmp":
+        return None, (a > b) - (a < b)
+    if op == "is_zero":
+        return None, int(a == 0)
+    if op == "is_one":
+        return None, int(a == 1)
+    if op == "cmov":
+        return (a if arg & 1 else c), 0
+    if op == "is_qr":
+        return None, int(a == 0 or pow(a, (P - 1) // 2, P) == 1)
+    if op == "sqrt":  # src/fp.cu fp_sqrt: a^((p+1)/4), p = 3 mod 4
+        if a == 0:
+            return 0, 1
+        if pow(a, (P - 1) // 2, P) != 1:
+            return 0, 0
+        r = pow(a, (P + 1) // 4, P)
+        if r * r % P == a:
+            return r, 1
+        alt = (P - r) % P
+        return (alt, 1) if alt * alt % P == a else (r, 0)
+    if op == "pow_u64":
+        return pow(a, arg, P), 0
+    raise ValueError(op)
+
+
+def fp2_elem(op, a=(0, 0), b=(0, 0), c=(0, 0), arg=0):
+    """One Fp2 operation; mul/square/inv/div on standard form (src/fp2.cu)."""
+    def inv0(x):
+        return (0, 0) if x == (0, 0) else f2_inv(x)
+
+    if op == "add":
+        return f2_add(a, b), 0
+    if op == "sub":
+        return f2_sub(a, b), 0
+    if op == "mul":
+        return f2_mul(a, b), 0
+    if op == "square":
+        return f2_mul(a, a), 0
+    if op == "neg":
+        return ((-a[0]) % P, (-a[1]) % P), 0
+    if op in ("conjugate", "frobenius"):
+        return (a[0], (-a[1]) % P), 0
+    if op == "inv":
+        return inv0(a), 0
+    if op == "div":
+        return f2_mul(a, inv0(b)), 0
+    if op == "copy":
+        return a, 0
+    if op == "mul_by_i":
+        return ((-a[1]) % P, a[0]), 0
+    if op == "cmp":
+        d = (a[0] > b[0]) - (a[0] < b[0])
+        return None, d if d else (a[1] > b[1]) - (a[1] < b[1])
+    if op == "is_zero":
+        return None, int(a == (0, 0))
+    if op == "is_one":
+        return None, int(a == (1, 0))
+    if op == "cmov":
+        return (a if arg & 1 else c), 0
+    if op == "mont_mul":
+        m = f2_mul(a, b)
+        return (m[0] * R_INV % P, m[1] * R_INV % P), 0
+    raise ValueError(op)
+
+
+def point_elem(op, p, q=None, k=0, group=1):
+    """One affine point operation on (x, y, infinity) triples in standard
+    form, in the reference's branch order (src/curve.cu:72-268).  Montgomery
+    form commutes with these formulas, so the Montgomery-form result is the
+    conversion of this one."""
+    F = _field(group)
+    inf = (F.zero, F.zero, True)
+
+    def inv0(v):
+        return F.zero if v == F.zero else F.inv(v)
+
+    def dbl(pt):
+        x, y, i = pt
+        if i or y == F.zero:
+            return inf
+        lam = F.mul(inv0(F.add(y, y)), F.add(F.add(F.mul(x, x), F.mul(x, x)), F.mul(x, x)))
+        x3 = F.sub(F.mul(lam, lam), F.add(x, x))
+        return (x3, F.sub(F.mul(lam, F.sub(x, x3)), y), False)
+
+    def add(p1, p2):
+        if p1[2]:
+            return p2
+        if p2[2]:
+            return p1
+        (x1, y1, _), (x2, y2, _) = p1, p2
+        if x1 == x2 and y1 == F.neg(y2):
+            return inf
+        if x1 == x2 and y1 == y2:
+            return dbl(p1)
+        lam = F.mul(inv0(F.sub(x2, x1)), F.sub(y2, y1))
+        x3 = F.sub(F.sub(F.mul(lam, lam), x1), x2)
+        return (x3, F.sub(F.mul(lam, F.sub(x1, x3)), y1), False)
+
+    if op == "add":
+        return add(p, q)
+    if op == "double":
+        return dbl(p)
+    if op == "neg":
+        return inf if p[2] else (p[0], F.neg(p[1]), False)
+    if op in ("scalar_mul", "scalar_mul_u64"):  # MSB-first double-and-add, src/curve.cu:230
+        acc = inf
+        if p[2]:
+            return inf
+        for bit in reversed(range(max(k.bit_length(), 1))):
+            acc = dbl(acc)
+            if (k >> bit) & 1:
+                acc = add(acc, p)
+        return acc
+    if op == "at_infinity":
+        return inf
+    raise ValueError(op)

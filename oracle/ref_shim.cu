@@ -13,9 +13,44 @@
 // are accumulated in parallel by std::thread; the combine is serial.
 #include "src/curve.cu"
 
+#include <string>
 #include <thread>
 #include <vector>
 
+// point_to/from_montgomery are kernels in the reference
+// (src/curve.cu:2313-2340); their host-function bodies, through the same traits
+template <class P>
+void ref_point_convert(P &r, const P &p, bool to) {
+  using Tr = PointTraits<P>;
+  if (p.infinity) {
+    r.infinity = true;
+    Tr::field_zero(r.x);
+    Tr::field_zero(r.y);
+  } else if (to) {
+    Tr::field_to_montgomery(r.x, p.x);
+    Tr::field_to_montgomery(r.y, p.y);
+    r.infinity = false;
+  } else {
+    Tr::field_from_montgomery(r.x, p.x);
+    Tr::field_from_montgomery(r.y, p.y);
+    r.infinity = false;
+  }
+}
+
+template <class P>
+int ref_point_elem(const char *op, P *r, const P *p, const P *q, const uint64_t *k, int limbs, uint64_t k64) {
+  const std::string o(op);
+  if (o == "add") point_add(*r, *p, *q);
+  else if (o == "double") point_double(*r, *p);
+  else if (o == "neg") point_neg(*r, *p);
+  else if (o == "scalar_mul") point_scalar_mul(*r, *p, k, limbs);
+  else if (o == "scalar_mul_u64") point_scalar_mul(*r, *p, &k64, 1);
+  else if (o == "to_mont") ref_point_convert(*r, *p, true);
+  else if (o == "from_mont") ref_point_convert(*r, *p, false);
+  else if (o == "at_infinity") PointTraits<P>::point_at_infinity(*r);
+  else return -99;
+  return 0;
+}
 extern "C" {
 
 void ref_fp_mont_mul_batch(Fp *c, const Fp *a, const Fp *b, int64_t n) {
@@ -134,6 +169,67 @@ void ref_g2_msm_pippenger(G2Point *r, G2ProjectivePoint *r_proj, const G2Point *
     combine_buckets_cpu_projective_g2(res, &buckets[(size_t)w * MSM_BUCKET_COUNT], MSM_BUCKET_COUNT, w);
   if (r_proj) *r_proj = res;
   projective_to_affine_g2(*r, res);
+}
+
+// Single-element operations by name: the reference's __host__ __device__
+// functions that its stream-API kernels call (src/fp_kernels.cu:57-148,
+// src/fp2_kernels.cu:40-110, src/curve.cu:2288-2380).  Returns the value of
+// the predicates (cmp, is_zero, is_one, is_qr, sqrt), else 0; -99 for an
+// unknown name.
+int ref_fp_elem(const char *op, Fp *c, const Fp *a, const Fp *b, uint64_t arg) {
+  const std::string o(op);
+  if (o == "add") fp_add(*c, *a, *b);
+  else if (o == "sub") fp_sub(*c, *a, *b);
+  else if (o == "mul") fp_mul(*c, *a, *b);
+  else if (o == "neg") fp_neg(*c, *a);
+  else if (o == "inv") fp_inv(*c, *a);
+  else if (o == "div") fp_div(*c, *a, *b);
+  else if (o == "copy") fp_copy(*c, *a);
+  else if (o == "zero") fp_zero(*c);
+  else if (o == "one") fp_one(*c);
+  else if (o == "to_mont") fp_to_montgomery(*c, *a);
+  else if (o == "from_mont") fp_from_montgomery(*c, *a);
+  else if (o == "mont_mul") fp_mont_mul(*c, *a, *b);
+  else if (o == "cmp") return fp_cmp(*a, *b);
+  else if (o == "is_zero") return fp_is_zero(*a);
+  else if (o == "is_one") return fp_is_one(*a);
+  else if (o == "cmov") fp_cmov(*c, *a, arg);
+  else if (o == "sqrt") return fp_sqrt(*c, *a);
+  else if (o == "is_qr") return fp_is_quadratic_residue(*a);
+  else if (o == "pow_u64") fp_pow_u64(*c, *a, arg);
+  else return -99;
+  return 0;
+}
+
+int ref_fp2_elem(const char *op, Fp2 *c, const Fp2 *a, const Fp2 *b, uint64_t arg) {
+  const std::string o(op);
+  if (o == "add") fp2_add(*c, *a, *b);
+  else if (o == "sub") fp2_sub(*c, *a, *b);
+  else if (o == "mul") fp2_mul(*c, *a, *b);
+  else if (o == "square") fp2_square(*c, *a);
+  else if (o == "neg") fp2_neg(*c, *a);
+  else if (o == "conjugate") fp2_conjugate(*c, *a);
+  else if (o == "inv") fp2_inv(*c, *a);
+  else if (o == "div") fp2_div(*c, *a, *b);
+  else if (o == "copy") fp2_copy(*c, *a);
+  else if (o == "mul_by_i") fp2_mul_by_i(*c, *a);
+  else if (o == "frobenius") fp2_frobenius(*c, *a);
+  else if (o == "cmp") return fp2_cmp(*a, *b);
+  else if (o == "is_zero") return fp2_is_zero(*a);
+  else if (o == "is_one") return fp2_is_one(*a);
+  else if (o == "cmov") fp2_cmov(*c, *a, arg);
+  else if (o == "mont_mul") fp2_mont_mul(*c, *a, *b);
+  else return -99;
+  return 0;
+}
+
+int ref_g1_point_elem(const char *op, G1Point *r, const G1Point *p, const G1Point *q, const uint64_t *k, int limbs,
+                      uint64_t k64) {
+  return ref_point_elem(op, r, p, q, k, limbs, k64);
+}
+int ref_g2_point_elem(const char *op, G2Point *r, const G2Point *p, const G2Point *q, const uint64_t *k, int limbs,
+                      uint64_t k64) {
+  return ref_point_elem(op, r, p, q, k, limbs, k64);
 }
 
 }  // extern "C"

@@ -41,7 +41,7 @@ def test_library_exports_reference_cxx_api():
     L = gm.lib()
     path = os.path.join(ROOT, "tests", "golden", "cxx_symbols.txt")
     syms = [s.strip() for s in open(path) if s.strip() and not s.startswith("#")]
-    assert len(syms) >= 20
+    assert len(syms) >= 120
     missing = [s for s in syms if not hasattr(L, s)]
     assert not missing, missing
 

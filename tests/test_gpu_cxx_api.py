@@ -91,3 +91,40 @@ def test_cxx_api_matches_oracle(cuda, tmp_path):
     assert np.array_equal(rd("out_fp2_mul_host.bin", np.uint64).reshape(a2.shape), oracle.fp2_mul(a2, b2))
     want2 = np.stack([want_add[:100], want_add[100:200]], axis=1)
     assert np.array_equal(rd("out_fp2_add_host.bin", np.uint64).reshape(a2.shape), want2)
+
+    # single-element stream APIs and host-pointer helpers (fp.h:158-204,
+    # fp2.h:99-133, curve.h:156-205, fp_kernels.h:26-38, fp2_kernels.h:21-37)
+    from tests import element_cases as ec
+    x, y = xs[0], ys[0]
+    fe = lambda op, a=0, b=0, c=0, arg=0: pyref.fp_elem(op, a, b, c, arg)[0]  # noqa: E731
+    want_fp = [fe("add", x, y), fe("sub", x, y), fe("mul", x, y), fe("div", x, y), fe("mont_mul", x, y),
+               fe("neg", x), fe("inv", x), fe("to_mont", x), fe("from_mont", x), x, 0, 1,
+               fe("add", x, y), fe("sub", x, y), fe("mul", x, y), fe("neg", x), fe("inv", x), fe("div", x, y),
+               fe("to_mont", x), fe("from_mont", x), fe("mont_mul", x, y), x, x, y, fe("pow_u64", x, arg=65537),
+               fe("sqrt", x * x % P)]
+    got_fp = rd("out_elem_fp.bin", np.uint64).reshape(-1, 7)
+    assert [ec.fp_int(r) for r in got_fp] == want_fp
+    x2, y2 = (xs[0], xs[100]), (ys[0], ys[100])
+    f2 = lambda op, a, b=(0, 0): pyref.fp2_elem(op, a, b)[0]  # noqa: E731
+    want_fp2 = [f2("add", x2, y2), f2("sub", x2, y2), f2("mul", x2, y2), f2("div", x2, y2), f2("square", x2),
+                f2("neg", x2), f2("conjugate", x2), f2("inv", x2), x2,
+                f2("add", x2, y2), f2("sub", x2, y2), f2("mul", x2, y2), f2("neg", x2), f2("conjugate", x2),
+                f2("square", x2), f2("inv", x2), f2("div", x2, y2), f2("mul_by_i", x2), f2("frobenius", x2), x2,
+                x2]
+    got_fp2 = rd("out_elem_fp2.bin", np.uint64).reshape(-1, 14)
+    assert [ec.fp2_int(r) for r in got_fp2] == want_fp2
+    want_flags = [1, pyref.fp_elem("cmp", x, y)[1], int(x == 0), 1, pyref.fp_elem("is_qr", x)[1],
+                  pyref.fp2_elem("cmp", x2, y2)[1], 0, 0]
+    assert rd("out_elem_flags.bin", np.int32).tolist() == want_flags
+    for group, (pts, logs, k64, k5) in groups.items():
+        p0, p1 = ec.point_from_np(pts[0:1], group), ec.point_from_np(pts[1:2], group)
+        k5i = oracle.limbs_to_int(k5[0])
+        std0 = ec.point_from_np(oracle.from_mont(pts[:1], group), group)
+        want = [ec.expected_point("add", p0, p1, 0, 0, group), ec.expected_point("double", p0, None, 0, 0, group),
+                ec.expected_point("neg", p0, None, 0, 0, group),
+                ec.expected_point("scalar_mul_u64", p0, None, int(k64[0, 0]), 0, group),
+                ec.expected_point("scalar_mul", p0, None, k5i, 5, group),
+                ec.expected_point("to_mont", std0, None, 0, 0, group),
+                ec.expected_point("from_mont", p0, None, 0, 0, group)]
+        got = rd(f"out_elem_g{group}.bin", gm.G1 if group == 1 else gm.G2)
+        assert [ec.point_from_np(got[i:i + 1], group) for i in range(7)] == want, group
