@@ -65,6 +65,7 @@ C_API = [
     "gm_batch_plan_run", "gm_batch_plan_destroy", "gm_batch_plan_bytes", "gm_batch_plan_classes",
     "gm_batch_run", "gm_batch_workspace_bytes", "gm_g1_sum_projective_host",
     "gm_host_selftest", "gm_fp_elem", "gm_fp2_elem", "gm_g1_point_elem", "gm_g2_point_elem",
+    "gm_g1_on_curve_batch", "gm_g2_on_curve_batch",
 ]
 
 
@@ -133,6 +134,8 @@ def lib() -> ctypes.CDLL:
             getattr(L, name).argtypes = [vp, u32, i32, vp, vp, vp, ctypes.c_uint64, vp]
         for name in ("gm_g1_point_elem", "gm_g2_point_elem"):
             getattr(L, name).argtypes = [vp, u32, i32, vp, vp, vp, vp, i32, ctypes.c_uint64]
+        for name in ("gm_g1_on_curve_batch", "gm_g2_on_curve_batch"):
+            getattr(L, name).argtypes = [vp, u32, vp, i64, vp]
         _lib = L
     return _lib
 
@@ -500,6 +503,19 @@ def point_elem(op: str, p=None, q=None, scalar=None, scalar_u64: int = 0, group:
               _ptr_or_null(q), _ptr_or_null(scalar), limbs, ctypes.c_uint64(scalar_u64 & 0xFFFFFFFFFFFFFFFF)),
            f"g{group}_point_{op}")
     return out
+
+
+def on_curve(points, group: int = 1, stream=None):
+    """uint8 device tensor (n,): 1 where the affine point (int64 device tensor
+    (n, 15) [G1Point] or (n, 29) [G2Point], Montgomery form) satisfies
+    y^2 = x^3 + 1 (G1) / x^3 + (1 + i) (G2) or is at infinity."""
+    import torch
+    _require(points, G1_WORDS if group == 1 else G2_WORDS, "points")
+    ok = torch.empty(points.shape[0], dtype=torch.uint8, device=points.device)
+    fn = lib().gm_g1_on_curve_batch if group == 1 else lib().gm_g2_on_curve_batch
+    _check(fn(_stream_handle(stream), _dev_index(points), ctypes.c_void_p(points.data_ptr()), points.shape[0],
+              ctypes.c_void_p(ok.data_ptr())), "on_curve")
+    return ok
 
 
 def to_numpy_points(t, group: int = 1) -> np.ndarray:

@@ -328,6 +328,16 @@ int gm_g1_point_elem(gm_stream_t stream, uint32_t gpu_index, int op, G1Point *d_
 int gm_g2_point_elem(gm_stream_t stream, uint32_t gpu_index, int op, G2Point *d_r, const G2Point *d_p,
                      const G2Point *d_q, const uint64_t *d_scalar, int scalar_limbs, uint64_t scalar_u64);
 
+/* d_ok[i] = 1 when affine point i (Montgomery form, device pointers) lies on
+ * the curve -- y^2 = x^3 + 1 (G1), y^2 = x^3 + (1 + i) (G2), the equations
+ * the reference's generators satisfy -- or carries the infinity flag; else 0.
+ * The reference's is_on_curve_g1/g2 (include/curve.h:53-59) are host/device
+ * inline functions with b = 4 / 4i, which reject its own generators; this
+ * batched check uses the corrected constants.  Validates bases before they
+ * become a resident table. */
+int gm_g1_on_curve_batch(gm_stream_t stream, uint32_t gpu_index, const G1Point *d_points, int64_t n, uint8_t *d_ok);
+int gm_g2_on_curve_batch(gm_stream_t stream, uint32_t gpu_index, const G2Point *d_points, int64_t n, uint8_t *d_ok);
+
 /* Host-side sum of n G1 projective points (Montgomery form): combines the
  * partial results of a sharded MSM on a CPU; no reference counterpart. */
 int gm_g1_sum_projective_host(G1ProjectivePoint *out, const G1ProjectivePoint *in, int n);

@@ -80,3 +80,31 @@ def test_elem_rejects_bad_arguments(cuda):
     assert L.gm_fp2_elem(None, 0, gm.FP2_OPS.index("cmp"), None, None, None, 0, None) == -1
     assert L.gm_g1_point_elem(None, 0, 99, None, None, None, None, 0, 0) == -1
     assert L.gm_g2_point_elem(None, 0, gm.POINT_OPS.index("add"), None, None, None, None, 0, 0) == -1
+
+
+@pytest.mark.parametrize("group", [1, 2])
+def test_on_curve_batch(cuda, group):
+    """Batched on-curve check with the constants the generators satisfy
+    (b = 1, b' = 1 + i): multiples of G pass, infinity passes, points with a
+    perturbed coordinate fail; the verdicts equal the oracle's."""
+    from gpu_msm_b200 import workload as wl
+    from oracle import pyref as pr
+    n = 300
+    logs = wl.make_base_logs(n, seed=77 + group)
+    pts_t = gm.generator_mul_batch(torch.from_numpy(logs.view(np.int64)).to(cuda), group=group)
+    pts = gm.to_numpy_points(pts_t, group).copy()
+    bad = np.arange(n) % 3 == 1
+    for i in np.nonzero(bad)[0]:  # y += 1 (Montgomery one added to the first limb word set)
+        y = ec.point_from_np(pts[i:i + 1], group)
+        F = pr._field(group)
+        y1 = F.add(y[1], F.small(pr.to_mont(1)) if group == 1 else (pr.to_mont(1), 0))
+        pts[i:i + 1] = ec.point_np((y[0], y1, False), group)
+    pts["infinity"][::7] = 1
+    ok = gm.on_curve(torch.from_numpy(pts.view(np.uint64).view(np.int64).reshape(n, -1)).to(cuda), group=group)
+    got = ok.cpu().numpy()
+    want = []
+    for i in range(n):
+        x, y, inf = ec._std_pt(ec.point_from_np(pts[i:i + 1], group), group)
+        want.append(1 if inf or pr.on_curve((x, y), group) else 0)
+    assert got.tolist() == want
+    assert got.sum() < n and got.sum() > n // 2
