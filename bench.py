@@ -8,9 +8,11 @@ shard (weak scaling); the shards' partial sums are exchanged with one
 all_gather and added on the device, as a sharded MSM does.
 
 Keys beyond the driver contract:
-  roofline      the dominant kernel (bucket accumulation) against the
-                measured IMAD peak of this GPU (bound "imad": the path is
-                exact integer arithmetic; neither tensor cores nor HBM bound it)
+  roofline      the dominant kernel (bucket accumulation): its fixed op count
+                (798 IMAD-equivalents per Fp product) against the measured
+                mad.lo peak of this GPU (bound "imad": the path is exact
+                integer arithmetic, its G1 products computed on the FP64 pipe;
+                neither tensor cores nor HBM bound it)
   msm_roofline  the whole MSM against the same peak, with the fixed op count
   cpu_baseline  the reference's own host code (oracle/_ref) on the host cores
   extra         Fp 2^26 and G2 2^18 measurements, phase breakdown
@@ -175,6 +177,11 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
+# k_accumulate<Fp> at G1 2^20, from the ncu capture summarised in
+# profiles/k_accumulate_g1_2p20.md: DRAM bytes per launch and pipe utilisation
+ACC_TRAFFIC_NCU = 1.582e9
+ACC_PIPES_NCU = {"fp64": 0.470, "alu": 0.538, "fma": 0.069, "issue": 0.581}
+
 # CPU baseline: reference host code (or the oracle port) on a bounded sample
 # ---------------------------------------------------------------------------
 def cpu_baseline_run(points, scalars, threads):
@@ -340,12 +347,13 @@ def run_ours(args, rank, world, local_rank):
     if rank != 0:
         return
 
-    # IMAD ceilings of this GPU (project microbenchmark): mad.lo alone (the
-    # roofline peak) and the lo/hi mix (context)
+    # multiply-add ceilings of this GPU (project microbenchmark): mad.lo alone
+    # (the roofline peak), the lo/hi mix of an integer Montgomery product and
+    # fma.rn.f64 (the pipe the G1 Montgomery products run on), for context
     sink = torch.empty(148 * 8 * 256 * 4, dtype=torch.int32, device=dev)
     iters = 4096
     peaks = {}
-    for mode in (0, 1):
+    for mode in (0, 1, 2):
         gm.imad_probe(64, sink, mode=mode)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -357,9 +365,11 @@ def run_ours(args, rank, world, local_rank):
             torch.cuda.synchronize()
             best = max(best, cnt / (e0.elapsed_time(e1) / 1e3))
         peaks[mode] = best
-    # roofline denominator: the IMAD issue peak (mad.lo only).  The lo/hi mix
-    # of a Montgomery product runs below it (the hi halves take extra pipe
-    # time), so quoting against the lo-only peak is the conservative choice.
+    # roofline denominator: the IMAD issue peak (mad.lo only), against which
+    # the fixed op count (798 IMAD-equivalents per Fp product) is quoted.  The
+    # lo/hi mix of an integer Montgomery product runs well below it (the hi
+    # halves take extra pipe time); the G1 products run on the FP64 pipe
+    # instead (field_f64.cuh), which is how the kernel gets past that mix.
     imad_peak = peaks[1]
 
     acc_ms = phase_ms.get("accumulate", float("nan"))
@@ -379,12 +389,14 @@ def run_ours(args, rank, world, local_rank):
                      "peak": imad_peak / 1e12, "unit": "TIMAD/s", "frac": achieved / imad_peak,
                      # dram__bytes_read + dram__bytes_write of one launch, from the ncu
                      # capture summarised in profiles/k_accumulate_g1_2p20.md
-                     "traffic": 1.592e9,
+                     "traffic": ACC_TRAFFIC_NCU,
                      "traffic_unit": "bytes per launch (ncu)",
-                     "work": f"798 IMAD x 10 Fp mults x {entries} entries per launch",
+                     "work": f"798 IMAD-equivalents x 10 Fp mults x {entries} entries per launch",
                      "peak_source": "measured: gm_imad_probe mode 1 (independent mad.lo chains over all SMs)",
                      "peak_lo_hi_mix": peaks[0] / 1e12,
-                     "imad_pipe_busy_ncu": 0.883},
+                     "fp64_fma_peak": peaks[2] / 1e12,
+                     "products_on": "FP64 pipe (DFMA.RZ exact splits, int64 column sums)",
+                     "pipes_busy_ncu": ACC_PIPES_NCU},
         "msm_roofline": {"ops_imad": msm_ops, "achieved": msm_ops / (ms / 1e3) / 1e12,
                          "frac": msm_ops / (ms / 1e3) / imad_peak, "unit": "TIMAD/s"},
         "phases_ms": phase_ms,

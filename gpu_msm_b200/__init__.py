@@ -554,8 +554,8 @@ def launch_count_reset() -> int:
 
 
 def imad_probe(iters: int, sink, stream=None, mode: int = 0) -> int:
-    """Launch the IMAD throughput probe (mode 0: lo/hi mix, 1: lo only);
-    returns IMADs per launch."""
+    """Launch the multiply-add throughput probe (mode 0: mad.lo/mad.hi mix,
+    1: mad.lo only, 2: fma.rn.f64); returns instructions per launch."""
     import torch
     if not (isinstance(sink, torch.Tensor) and sink.is_cuda and sink.dtype == torch.int32):
         raise ValueError("sink: int32 CUDA tensor")

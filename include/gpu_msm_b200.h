@@ -350,10 +350,11 @@ int gm_g1_sum_projective_host(G1ProjectivePoint *out, const G1ProjectivePoint *i
  *   in `names`; clears the record.
  * gm_launch_count_reset: number of kernels this library launched from the
  *   calling thread since the previous call.
- * gm_imad_probe: launches a kernel of independent 32-bit IMAD chains over
- *   the whole GPU (mode 0: half mad.lo, half mad.hi, the mix of a Montgomery
- *   product; mode 1: mad.lo only); *imad_per_launch receives the IMAD count
- *   so that the caller can time it and derive the multiply-add ceiling. */
+ * gm_imad_probe: launches a kernel of independent multiply-add chains over
+ *   the whole GPU (mode 0: half mad.lo, half mad.hi, the mix of an integer
+ *   Montgomery product; mode 1: mad.lo only; mode 2: fma.rn.f64, the pipe of
+ *   the FP64 Montgomery product); *imad_per_launch receives the instruction
+ *   count so that the caller can time it and derive the ceiling. */
 int gm_profile_enable(int on);
 int gm_profile_collect(char *names, int names_len, float *ms, int max);
 int64_t gm_launch_count_reset(void);
