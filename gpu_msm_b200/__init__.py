@@ -65,7 +65,7 @@ C_API = [
     "gm_batch_plan_run", "gm_batch_plan_destroy", "gm_batch_plan_bytes", "gm_batch_plan_classes",
     "gm_batch_run", "gm_batch_workspace_bytes", "gm_g1_sum_projective_host",
     "gm_host_selftest", "gm_fp_elem", "gm_fp2_elem", "gm_g1_point_elem", "gm_g2_point_elem",
-    "gm_g1_on_curve_batch", "gm_g2_on_curve_batch",
+    "gm_g1_on_curve_batch", "gm_g2_on_curve_batch", "gm_g1_msm_host_async", "gm_g2_msm_host_async",
 ]
 
 
@@ -136,6 +136,8 @@ def lib() -> ctypes.CDLL:
             getattr(L, name).argtypes = [vp, u32, i32, vp, vp, vp, vp, i32, ctypes.c_uint64]
         for name in ("gm_g1_on_curve_batch", "gm_g2_on_curve_batch"):
             getattr(L, name).argtypes = [vp, u32, vp, i64, vp]
+        for name in ("gm_g1_msm_host_async", "gm_g2_msm_host_async"):
+            getattr(L, name).argtypes = [vp, u32, vp, vp, vp, i32, i32, i32, vp]
         _lib = L
     return _lib
 
@@ -201,6 +203,31 @@ def msm(points: np.ndarray, scalars: np.ndarray, group: int = 1, montgomery: boo
     _check(fn(_p(out), _p(pts), _p(sc), sc.shape[1], len(pts), gpu_index, 1 if montgomery else 0),
            f"{g}_msm_limbs_wrapper")
     return out
+
+
+def msm_host_async(points: np.ndarray, scalars: np.ndarray, result: np.ndarray, group: int = 1,
+                   montgomery: bool = True, gpu_index: int = 0, stream=None, err: np.ndarray = None):
+    """Enqueue a host-buffer MSM on a torch CUDA stream (gm_g{1,2}_msm_host_async)
+    and return at once.  points: structured G1/G2 array; scalars: uint64
+    (n, limbs); result: a one-element G1P/G2P array receiving the projective
+    sum; err: optional uint32 array of one element for the device check flag.
+    Keep every buffer alive and read result only after the stream has passed
+    the call.  Page-locked buffers (e.g. numpy views of pinned torch tensors)
+    let the copies overlap other GPU work."""
+    adt, pdt = (G1, G1P) if group == 1 else (G2, G2P)
+    pts = np.asarray(points)
+    if pts.dtype != adt or not pts.flags["C_CONTIGUOUS"]:
+        raise ValueError("points: contiguous G1/G2 structured array")
+    sc = np.asarray(scalars)
+    if sc.dtype != np.uint64 or sc.ndim != 2 or sc.shape[0] != len(pts) or not sc.flags["C_CONTIGUOUS"]:
+        raise ValueError("scalars: contiguous uint64 array (n, limbs)")
+    if result.dtype != pdt or result.size != 1 or not result.flags["C_CONTIGUOUS"]:
+        raise ValueError("result: one contiguous projective point")
+    if err is not None and (err.dtype != np.uint32 or err.size != 1):
+        raise ValueError("err: one uint32")
+    fn = lib().gm_g1_msm_host_async if group == 1 else lib().gm_g2_msm_host_async
+    _check(fn(_stream_handle(stream), gpu_index, _p(result), _p(pts), _p(sc), sc.shape[1], len(pts),
+              1 if montgomery else 0, _p(err) if err is not None else None), "msm_host_async")
 
 
 def g1_msm(points, scalars, montgomery=True, gpu_index=0):

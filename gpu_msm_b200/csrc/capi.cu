@@ -314,6 +314,91 @@ int host_msm(Prj *result, const Aff *points, const uint64_t *scalars, int limbs,
   return gm::GM_OK;
 }
 
+// One non-blocking helper stream per device for the points' copy of the
+// asynchronous host-buffer MSM (created on first use, kept for the process).
+std::mutex g_copy_mu;
+std::map<int, cudaStream_t> g_copy_streams;
+
+int copy_stream(int dev, cudaStream_t *out) {
+  std::lock_guard<std::mutex> lk(g_copy_mu);
+  auto it = g_copy_streams.find(dev);
+  if (it == g_copy_streams.end()) {
+    cudaStream_t cs;
+    if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) return gm::GM_ERR_STREAM;
+    it = g_copy_streams.emplace(dev, cs).first;
+  }
+  *out = it->second;
+  return gm::GM_OK;
+}
+
+// Host-buffer MSM enqueued on the caller's stream s: scalars copied on s,
+// points on the helper stream (so that their copy overlaps the sort), the
+// MSM, then the result (and the consistency flag) copied back to host
+// memory; nothing waits on the host.  Per-call events are released once
+// the stream has passed them.
+template <class F, class Aff, class Prj>
+int host_msm_async(cudaStream_t s, uint32_t gpu_index, Prj *result, const Aff *points, const uint64_t *scalars,
+                   int limbs, int n, int to_mont, uint32_t *err_flag) {
+  if (result == nullptr || n < 0 || (n > 0 && (points == nullptr || scalars == nullptr))) return gm::GM_ERR_ARG;
+  if (limbs < 1 || limbs > gm::MAX_SCALAR_LIMBS) return gm::GM_ERR_ARG;
+  int rc = gm::select_device(gpu_index);
+  if (rc) return rc;
+  const size_t pts_bytes = (size_t)n * sizeof(Aff), sc_bytes = (size_t)n * limbs * sizeof(uint64_t);
+  const size_t o_sc = (pts_bytes + 255) / 256 * 256;
+  const size_t o_res = o_sc + (sc_bytes + 255) / 256 * 256;
+  const size_t o_err = o_res + 512;
+  char *buf = nullptr;
+  rc = gm::pool_alloc((int)gpu_index, s, o_err + 256, (void **)&buf);
+  if (rc) return rc;
+  cudaError_t e = cudaSuccess;
+  if (n == 0) {  // the identity: Z = 0 (reference layout, all words zero)
+    e = cudaMemsetAsync(buf + o_res, 0, sizeof(Prj), s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(result, buf + o_res, sizeof(Prj), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && err_flag) e = cudaMemsetAsync(buf + o_err, 0, sizeof(uint32_t), s);
+    if (e == cudaSuccess && err_flag)
+      e = cudaMemcpyAsync(err_flag, buf + o_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    cudaFreeAsync(buf, s);
+    return e == cudaSuccess ? gm::GM_OK : gm::record_error(e, "host_msm_async");
+  }
+  cudaStream_t s2;
+  rc = copy_stream((int)gpu_index, &s2);
+  if (rc) {
+    cudaFreeAsync(buf, s);
+    return rc;
+  }
+  cudaEvent_t alloc_done, pts_done;
+  if (cudaEventCreateWithFlags(&alloc_done, cudaEventDisableTiming) != cudaSuccess) {
+    cudaFreeAsync(buf, s);
+    return gm::GM_ERR_STREAM;
+  }
+  if (cudaEventCreateWithFlags(&pts_done, cudaEventDisableTiming) != cudaSuccess) {
+    cudaEventDestroy(alloc_done);
+    cudaFreeAsync(buf, s);
+    return gm::GM_ERR_STREAM;
+  }
+  e = cudaMemcpyAsync(buf + o_sc, scalars, sc_bytes, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaEventRecord(alloc_done, s);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(s2, alloc_done, 0);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(buf, points, pts_bytes, cudaMemcpyHostToDevice, s2);
+  if (e == cudaSuccess) e = cudaEventRecord(pts_done, s2);
+  if (e == cudaSuccess) {
+    rc = gm::msm_launch<F>(s, (int)gpu_index, nullptr, (const uint64_t *)buf, to_mont, (const uint64_t *)(buf + o_sc),
+                           limbs, n, (uint64_t *)(buf + o_res), 0, (uint32_t *)(buf + o_err), pts_done);
+    if (rc == gm::GM_OK) {
+      e = cudaMemcpyAsync(result, buf + o_res, sizeof(Prj), cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess && err_flag)
+        e = cudaMemcpyAsync(err_flag, buf + o_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    }
+  }
+  // s waited for pts_done inside msm_launch, or waits here on an early error
+  cudaStreamWaitEvent(s, pts_done, 0);
+  cudaFreeAsync(buf, s);
+  cudaEventDestroy(alloc_done);
+  cudaEventDestroy(pts_done);
+  if (rc) return rc;
+  return e == cudaSuccess ? gm::GM_OK : gm::record_error(e, "host_msm_async");
+}
+
 }  // namespace
 
 extern "C" {
@@ -447,6 +532,18 @@ int g2_msm_limbs_wrapper(G2ProjectivePoint *result, const G2Point *points, const
                          int n, uint32_t gpu_index, int points_montgomery) {
   if (scalar_limbs < 1 || scalar_limbs > gm::MAX_SCALAR_LIMBS) return gm::GM_ERR_ARG;
   return host_msm<gm::Fp2>(result, points, scalars, scalar_limbs, n, gpu_index, points_montgomery ? 0 : 1);
+}
+
+int gm_g1_msm_host_async(gm_stream_t stream, uint32_t gpu_index, G1ProjectivePoint *result, const G1Point *points,
+                         const uint64_t *scalars, int scalar_limbs, int n, int points_montgomery, uint32_t *err_flag) {
+  return host_msm_async<gm::Fp>((cudaStream_t)stream, gpu_index, result, points, scalars, scalar_limbs, n,
+                                points_montgomery ? 0 : 1, err_flag);
+}
+
+int gm_g2_msm_host_async(gm_stream_t stream, uint32_t gpu_index, G2ProjectivePoint *result, const G2Point *points,
+                         const uint64_t *scalars, int scalar_limbs, int n, int points_montgomery, uint32_t *err_flag) {
+  return host_msm_async<gm::Fp2>((cudaStream_t)stream, gpu_index, result, points, scalars, scalar_limbs, n,
+                                 points_montgomery ? 0 : 1, err_flag);
 }
 
 int gm_g1_msm_device_c(gm_stream_t stream, uint32_t gpu_index, G1ProjectivePoint *d_result, const G1Point *d_points,

@@ -96,6 +96,23 @@ int g1_msm_limbs_wrapper(G1ProjectivePoint *result, const G1Point *points, const
 int g2_msm_limbs_wrapper(G2ProjectivePoint *result, const G2Point *points, const uint64_t *scalars,
                          int scalar_limbs, int n, uint32_t gpu_index, int points_montgomery);
 
+/* Host-buffer MSM, asynchronous on `stream`: the same computation as
+ * g{1,2}_msm_limbs_wrapper, enqueued instead of waited for.  The scalar and
+ * point copies from host memory, the MSM and the copy of the projective
+ * result to *result (host memory) are all ordered on `stream`; the call
+ * returns once they are enqueued.  The host buffers must stay valid, and
+ * *result unread, until the stream has passed the call (synchronise the
+ * stream or an event recorded after it).  With page-locked buffers the
+ * copies overlap other work on the GPU, e.g. the previous MSM on another
+ * stream; with pageable ones the copies block.  *err_flag (host, optional)
+ * receives the device consistency flag (0 = ok) in the same order.  No
+ * reference counterpart: the reference's host-buffer wrappers are
+ * synchronous (rust-api/src/c_wrapper.cu:64-258). */
+int gm_g1_msm_host_async(gm_stream_t stream, uint32_t gpu_index, G1ProjectivePoint *result, const G1Point *points,
+                         const uint64_t *scalars, int scalar_limbs, int n, int points_montgomery, uint32_t *err_flag);
+int gm_g2_msm_host_async(gm_stream_t stream, uint32_t gpu_index, G2ProjectivePoint *result, const G2Point *points,
+                         const uint64_t *scalars, int scalar_limbs, int n, int points_montgomery, uint32_t *err_flag);
+
 /* Device-pointer MSM, asynchronous on `stream`.  Replaces
  * point_msm_u64_async_g1/_g2 (include/curve.h:232-235; scalar_limbs = 1) and
  * point_msm_async<G1Point>/<G2Point> (include/curve.h:238) without the

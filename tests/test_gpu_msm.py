@@ -285,3 +285,47 @@ def test_plain_msm_graph_capture(cuda):
         got = oracle.proj_to_affine(gm.to_numpy_proj(out, 1), 1)
         assert oracle.same_point(got, oracle.generator_multiple(wl.expected_log(sc, logs)))
     del g
+
+
+@pytest.mark.parametrize("group", [1, 2])
+def test_host_async_two_streams(cuda, group):
+    """gm_g{1,2}_msm_host_async: several host-buffer MSMs in flight on two
+    streams (pinned buffers), each result equal to the exact relation; the
+    empty MSM gives the identity; bad arguments are rejected."""
+    import torch
+    streams = [torch.cuda.Stream(), torch.cuda.Stream()]
+    adt, pdt = (gm.G1, gm.G1P) if group == 1 else (gm.G2, gm.G2P)
+    words = gm.G1_WORDS if group == 1 else gm.G2_WORDS
+    pwords = gm.G1P_WORDS if group == 1 else gm.G2P_WORDS
+    cases = []
+    for i, n in enumerate((700, 3000, 1, 2500)):
+        logs = wl.make_base_logs(n, seed=800 + i + 10 * group)
+        sc = wl.make_scalars(n, seed=900 + i + 10 * group)
+        pts = make_bases(logs, group, cuda)
+        pts_pin = torch.empty((n, words), dtype=torch.int64, pin_memory=True)
+        pts_pin.copy_(pts.cpu())
+        sc_pin = torch.empty((n, 5), dtype=torch.int64, pin_memory=True)
+        sc_pin.copy_(torch.from_numpy(sc.view(np.int64)))
+        cases.append((pts_pin, sc_pin, oracle.generator_multiple(wl.expected_log(sc, logs), group=group)))
+    res = torch.zeros((len(cases) + 1, pwords), dtype=torch.int64, pin_memory=True)
+    err = torch.ones(len(cases) + 1, dtype=torch.int32, pin_memory=True)
+    res_np = res.numpy().view(np.uint64).view(pdt).reshape(-1)
+    err_np = err.numpy().view(np.uint32)
+    for i, (pts_pin, sc_pin, _) in enumerate(cases):
+        gm.msm_host_async(pts_pin.numpy().view(np.uint64).view(adt).reshape(-1), sc_pin.numpy().view(np.uint64),
+                          res_np[i:i + 1], group=group, stream=streams[i % 2], err=err_np[i:i + 1])
+    empty = np.zeros(0, dtype=adt)
+    k = len(cases)
+    res_np[k]["X"] = 5  # must be overwritten with the identity
+    gm.msm_host_async(empty, np.zeros((0, 5), dtype=np.uint64), res_np[k:k + 1], group=group, stream=streams[0],
+                      err=err_np[k:k + 1])
+    for s in streams:
+        s.synchronize()
+    assert err_np.max() == 0
+    for i, (_, _, want) in enumerate(cases):
+        assert oracle.same_point(oracle.proj_to_affine(res_np[i:i + 1], group), want), i
+    assert oracle.proj_to_affine(res_np[k:k + 1], group)[0]["infinity"]
+    L = gm.lib()
+    fn = L.gm_g1_msm_host_async if group == 1 else L.gm_g2_msm_host_async
+    assert fn(None, 0, None, None, None, 5, 10, 1, None) == -1
+    assert fn(None, 0, res_np[:1].ctypes.data, res_np[:1].ctypes.data, res_np[:1].ctypes.data, 9, 1, 1, None) == -1
