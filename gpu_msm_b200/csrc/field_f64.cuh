@@ -15,11 +15,14 @@
 //     the bit patterns of h and l are fixed constants plus H and L;
 //   - those bit patterns are summed as 64-bit integers into 18 columns of
 //     52 bits; each column later subtracts (number of terms) x constant once;
-//   - Montgomery reduction runs over the columns: eight steps with a 52-bit
-//     m = t * (-p^-1) mod 2^52 (one 64-bit integer product), then one step
-//     with a 32-bit m, which clears 8*52 + 32 = 448 bits.  A step's carry is
-//     (t >> 52) + (t mod 2^52 != 0), because t + lo(m*p0) is a multiple of
-//     2^52, so lo(m*p0) itself is never formed;
+//   - Montgomery reduction interleaves with the product in operand-scanning
+//     order: row i of a*b completes column i, then step i clears it.  Eight
+//     steps use a 52-bit m = t * (-p^-1) mod 2^52 (one 64-bit integer
+//     product), a last one a 32-bit m, which clears 8*52 + 32 = 448 bits.  A
+//     step's carry is (t >> 52) + (t mod 2^52 != 0), because t + lo(m*p0) is
+//     a multiple of 2^52, so lo(m*p0) itself is never formed.  (The
+//     interleaved order keeps fewer columns live than forming all of a*b
+//     first: G1 2^20 accumulation 11.10 ms against 11.24 ms.)
 //   - the result is the columns from bit 448 up, shifted into 14 x 32-bit
 //     limbs, below 2p, then one conditional subtraction of p.
 // Column sums stay below 36 * 2^52 < 2^58, so no column overflows.
@@ -106,21 +109,19 @@ GM_DEVI void split_acc(double a, double b, uint64_t &lo, uint64_t &hi) {
 }
 
 GM_DEVI void mont_mul(uint32_t r[NL], const uint32_t a[NL], const uint32_t b[NL]) {
-  double ad[9], bd[9];
+  double bd[9];
 #pragma unroll
-  for (int i = 0; i < 9; i++) {
-    ad[i] = to_d(limb52(a, i));
-    bd[i] = to_d(limb52(b, i));
-  }
+  for (int i = 0; i < 9; i++) bd[i] = to_d(limb52(b, i));
   uint64_t col[18];
 #pragma unroll
   for (int k = 0; k < 18; k++) col[k] = 0;
-#pragma unroll
-  for (int i = 0; i < 9; i++)
-#pragma unroll
-    for (int j = 0; j < 9; j++) split_acc(ad[i], bd[j], col[i + j], col[i + j + 1]);
+  // operand scanning: row i of a*b completes column i, then reduction step
+  // i clears it (columns i+1 .. i+9 are the only live ones)
 #pragma unroll
   for (int i = 0; i < 8; i++) {
+    const double ai = to_d(limb52(a, i));
+#pragma unroll
+    for (int j = 0; j < 9; j++) split_acc(ai, bd[j], col[i + j], col[i + j + 1]);
     const uint64_t t = col[i] - offset(i, i, false);  // exact value of column i
     const uint64_t tl = t & MASK52;
     const double m = to_d((tl * PINV52) & MASK52);
@@ -128,6 +129,11 @@ GM_DEVI void mont_mul(uint32_t r[NL], const uint32_t a[NL], const uint32_t b[NL]
     col[i + 1] += as_u(__fma_rz(m, (double)p52(0), 0x1p104));
 #pragma unroll
     for (int j = 1; j < 9; j++) split_acc(m, (double)p52(j), col[i + j], col[i + j + 1]);
+  }
+  {
+    const double a8 = to_d(limb52(a, 8));
+#pragma unroll
+    for (int j = 0; j < 9; j++) split_acc(a8, bd[j], col[8 + j], col[9 + j]);
   }
   // last step: a 32-bit m clears bits 416..447
   const uint64_t t8 = col[8] - offset(8, 8, false);

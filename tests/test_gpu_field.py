@@ -80,6 +80,28 @@ def test_fp_edges(cuda):
     assert np.array_equal(run("fp_mont_mul", a, b, cuda), oracle.fp_mont_mul(a, b))
 
 
+def test_fp_mont_mul_limb52_patterns(cuda):
+    """The FP64-pipe product works on 52-bit limbs: operands whose 52-bit
+    limbs sit at the split boundaries (all ones, zero, single high bits,
+    values just below p in each limb position) against the oracle, both
+    orders, bit-exact; also the G1 accumulation path's out-of-line product
+    through a full MSM is covered by the MSM tests."""
+    P = pyref.P
+    M = (1 << 52) - 1
+    pats = [0, 1, M, 1 << 51, (1 << 52) - 2, P - 1, P - 2, P >> 1, (P + 1) // 2]
+    for k in range(9):
+        pats += [(1 << (52 * k)) - 1, 1 << (52 * k), (M << (52 * k)) % P, P - (1 << (52 * k))]
+        pats += [sum(M << (52 * i) for i in range(k + 1)) % P]
+    pats += [(1 << 446) - 1 if (1 << 446) - 1 < P else P - 7, ((1 << 416) - 1), (P >> 416) << 416]
+    pats = sorted({v % P for v in pats})
+    xs = [x for x in pats for _ in pats]
+    ys = [y for _ in pats for y in pats]
+    a, b = oracle.ints_to_fp_array(xs), oracle.ints_to_fp_array(ys)
+    want = oracle.ints_to_fp_array([x * y * pow(1 << 448, -1, P) % P for x, y in zip(xs, ys)])
+    assert np.array_equal(run("fp_mont_mul", a, b, cuda), want)
+    assert np.array_equal(run("fp_mont_mul", a, b, cuda), oracle.fp_mont_mul(a, b))
+
+
 def test_fp2_random(cuda):
     rng = np.random.default_rng(2)
     a = rng.integers(0, 2 ** 64, size=(4096, 2, 7), dtype=np.uint64)
