@@ -179,8 +179,8 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # k_accumulate<Fp> at G1 2^20, from the ncu capture summarised in
 # profiles/k_accumulate_g1_2p20.md: DRAM bytes per launch and pipe utilisation
-ACC_TRAFFIC_NCU = 1.582e9
-ACC_PIPES_NCU = {"fp64": 0.470, "alu": 0.538, "fma": 0.069, "issue": 0.581}
+ACC_TRAFFIC_NCU = 1.586e9
+ACC_PIPES_NCU = {"fp64": 0.476, "alu": 0.545, "fma": 0.072, "issue": 0.589}
 
 # CPU baseline: reference host code (or the oracle port) on a bounded sample
 # ---------------------------------------------------------------------------

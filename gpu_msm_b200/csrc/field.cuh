@@ -270,6 +270,63 @@ GM_DEVI void mont_mul_raw(uint32_t r[NL], const uint32_t a[NL], const uint32_t b
 }
 
 // ---------------------------------------------------------------------------
+// Montgomery reduction of a 28-word value T < p * R: r = T * R^-1 mod p
+// (below 2p before the optional final subtraction).  X holds the low half of
+// T plus the even quotient products, Y the odd ones (one word up); the high
+// half of T is added at the end.
+// ---------------------------------------------------------------------------
+template <bool STRICT>
+GM_DEVI void redc_wide(uint32_t r[NL], const uint32_t T[2 * NL]) {
+  uint32_t X[2 * NL], Y[2 * NL];
+#pragma unroll
+  for (int k = 0; k < NL; k++) {
+    X[k] = T[k];
+    Y[k] = 0;
+  }
+  uint32_t c = 0;
+#pragma unroll
+  for (int i = 0; i < NL; i++) {
+    const uint32_t u = (i == 0) ? X[0] : X[i] + Y[i - 1] + c;
+    const uint32_t m = u * FpConst::PINV;
+    X[i] = mad_lo_cc(m, FpConst::P(0), X[i]);
+    X[i + 1] = madc_hi_cc(m, FpConst::P(0), X[i + 1]);
+#pragma unroll
+    for (int j = 2; j < NL; j += 2) {
+      X[i + j] = madc_lo_cc(m, FpConst::P(j), X[i + j]);
+      X[i + j + 1] = madc_hi_cc(m, FpConst::P(j), X[i + j + 1]);
+    }
+    X[i + NL] = addc(0, 0);
+    Y[i] = mad_lo_cc(m, FpConst::P(1), Y[i]);
+    Y[i + 1] = madc_hi_cc(m, FpConst::P(1), Y[i + 1]);
+#pragma unroll
+    for (int j = 3; j < NL; j += 2) {
+      Y[i + j - 1] = madc_lo_cc(m, FpConst::P(j), Y[i + j - 1]);
+      Y[i + j] = madc_hi_cc(m, FpConst::P(j), Y[i + j]);
+    }
+    Y[i + NL] = addc(0, 0);
+    if (i == 0) {
+      c = 0;
+    } else {
+      uint32_t t = add_cc(X[i], Y[i - 1]);
+      uint32_t c1 = addc(0, 0);
+      t = add_cc(t, c);
+      c = addc(c1, 0);
+      (void)t;
+    }
+  }
+  r[0] = add_cc(X[NL], Y[NL - 1]);
+#pragma unroll
+  for (int k = 1; k < NL; k++) r[k] = addc_cc(X[NL + k], Y[NL - 1 + k]);
+  r[0] = add_cc(r[0], c);
+#pragma unroll
+  for (int k = 1; k < NL; k++) r[k] = addc_cc(r[k], 0);
+  r[0] = add_cc(r[0], T[NL]);
+#pragma unroll
+  for (int k = 1; k < NL; k++) r[k] = addc_cc(r[k], T[NL + k]);
+  if (STRICT) cond_sub<false>(r);
+}
+
+// ---------------------------------------------------------------------------
 // Montgomery squaring (separated operand scanning): the 91 cross products
 // a_i*a_j (i < j) are formed once, doubled by a one-bit shift, and the 14
 // squares a_i^2 are added on the diagonal; the 28-word square is then reduced
@@ -335,55 +392,7 @@ GM_DEVI void mont_sqr_raw(uint32_t r[NL], const uint32_t a[NL]) {
     T[2 * i] = madc_lo_cc(a[i], a[i], T[2 * i]);
     T[2 * i + 1] = madc_hi_cc(a[i], a[i], T[2 * i + 1]);
   }
-  // reduction: X = low half of T plus the even quotient products, Y the odd
-  // ones (one word up); the high half of T is added at the end
-  uint32_t X[2 * NL], Y[2 * NL];
-#pragma unroll
-  for (int k = 0; k < NL; k++) {
-    X[k] = T[k];
-    Y[k] = 0;
-  }
-  uint32_t c = 0;
-#pragma unroll
-  for (int i = 0; i < NL; i++) {
-    const uint32_t u = (i == 0) ? X[0] : X[i] + Y[i - 1] + c;
-    const uint32_t m = u * FpConst::PINV;
-    X[i] = mad_lo_cc(m, FpConst::P(0), X[i]);
-    X[i + 1] = madc_hi_cc(m, FpConst::P(0), X[i + 1]);
-#pragma unroll
-    for (int j = 2; j < NL; j += 2) {
-      X[i + j] = madc_lo_cc(m, FpConst::P(j), X[i + j]);
-      X[i + j + 1] = madc_hi_cc(m, FpConst::P(j), X[i + j + 1]);
-    }
-    X[i + NL] = addc(0, 0);
-    Y[i] = mad_lo_cc(m, FpConst::P(1), Y[i]);
-    Y[i + 1] = madc_hi_cc(m, FpConst::P(1), Y[i + 1]);
-#pragma unroll
-    for (int j = 3; j < NL; j += 2) {
-      Y[i + j - 1] = madc_lo_cc(m, FpConst::P(j), Y[i + j - 1]);
-      Y[i + j] = madc_hi_cc(m, FpConst::P(j), Y[i + j]);
-    }
-    Y[i + NL] = addc(0, 0);
-    if (i == 0) {
-      c = 0;
-    } else {
-      uint32_t t = add_cc(X[i], Y[i - 1]);
-      uint32_t c1 = addc(0, 0);
-      t = add_cc(t, c);
-      c = addc(c1, 0);
-      (void)t;
-    }
-  }
-  r[0] = add_cc(X[NL], Y[NL - 1]);
-#pragma unroll
-  for (int k = 1; k < NL; k++) r[k] = addc_cc(X[NL + k], Y[NL - 1 + k]);
-  r[0] = add_cc(r[0], c);
-#pragma unroll
-  for (int k = 1; k < NL; k++) r[k] = addc_cc(r[k], 0);
-  r[0] = add_cc(r[0], T[NL]);
-#pragma unroll
-  for (int k = 1; k < NL; k++) r[k] = addc_cc(r[k], T[NL + k]);
-  if (STRICT) cond_sub<false>(r);
+  redc_wide<STRICT>(r, T);
 }
 
 // ---------------------------------------------------------------------------
