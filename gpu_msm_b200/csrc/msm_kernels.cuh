@@ -550,7 +550,10 @@ struct StagedPoint {
 // hit consecutive banks.  Only the owning thread reads its slots, so no
 // block-level barrier is needed.
 template <class F>
-__global__ void __launch_bounds__(ACC_THREADS) k_accumulate(const uint4 *__restrict__ bases, const uint32_t *__restrict__ entries,
+#ifndef GM_ACC_MIN_BLOCKS
+#define GM_ACC_MIN_BLOCKS 1
+#endif
+__global__ void __launch_bounds__(ACC_THREADS, GM_ACC_MIN_BLOCKS) k_accumulate(const uint4 *__restrict__ bases, const uint32_t *__restrict__ entries,
                                                     const uint32_t *__restrict__ offsets, int64_t K, int64_t nthreads,
                                                     xyzz_t<F> *__restrict__ buckets,
                                                     xyzz_t<F> *__restrict__ part_head, xyzz_t<F> *__restrict__ part_tail,
