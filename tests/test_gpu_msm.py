@@ -329,3 +329,26 @@ def test_host_async_two_streams(cuda, group):
     fn = L.gm_g1_msm_host_async if group == 1 else L.gm_g2_msm_host_async
     assert fn(None, 0, None, None, None, 5, 10, 1, None) == -1
     assert fn(None, 0, res_np[:1].ctypes.data, res_np[:1].ctypes.data, res_np[:1].ctypes.data, 9, 1, 1, None) == -1
+
+
+@pytest.mark.parametrize("group,n", [(1, (1 << 24) - 3), (2, (1 << 21) + 5)])
+def test_max_size_exact_relation(cuda, group, n):
+    """Well past the benchmark sizes, with ragged n: 2^24 - 3 G1 points and
+    2^21 + 5 G2 points against the exact relation sum k_i t_i (mod r), and
+    linearity: the MSM of the whole equals the sum of the MSMs of two
+    unequal parts."""
+    import torch
+    sc = wl.make_scalars(n, seed=7000 + group)
+    logs = wl.make_base_logs(n, seed=7100 + group)
+    pts = make_bases(logs, group, cuda)
+    sc_t = t_dev(sc, cuda).reshape(n, -1)
+    got = device_msm(pts, sc_t, group, cuda)
+    want = oracle.generator_multiple(wl.expected_log(sc, logs), group=group)
+    assert oracle.same_point(got, want)
+    cut = n // 3
+    a = gm.msm_device(pts[:cut].contiguous(), sc_t[:cut].contiguous(), group=group)
+    b = gm.msm_device(pts[cut:].contiguous(), sc_t[cut:].contiguous(), group=group)
+    both = torch.stack([a, b])
+    s = gm.sum_projective(both, group=group)
+    torch.cuda.synchronize()
+    assert oracle.same_point(oracle.proj_to_affine(gm.to_numpy_proj(s, group), group), want)
