@@ -9,13 +9,13 @@ all_gather and added on the device, as a sharded MSM does.
 
 Keys beyond the driver contract:
   roofline      the dominant kernel (bucket accumulation): its fixed op count
-                (798 IMAD-equivalents per Fp product) against the measured
-                mad.lo peak of this GPU (bound "imad": the path is exact
-                integer arithmetic, its G1 products computed on the FP64 pipe;
+                (798 IMAD per Fp product) against the measured mad.lo peak of
+                this GPU (bound "imad": the path is exact integer arithmetic;
                 neither tensor cores nor HBM bound it)
   msm_roofline  the whole MSM against the same peak, with the fixed op count
   cpu_baseline  the reference's own host code (oracle/_ref) on the host cores
-  extra         Fp 2^26 and G2 2^18 measurements, phase breakdown
+  extra         Fp 2^26 and G2 2^18 measurements, phase breakdown, the
+                optional FP64-product mode of the G1 accumulation
 
 --impl reference times the reference's CPU implementation of the path
 (oracle/_ref, all host threads) on a bounded sample of the same workload.
@@ -177,10 +177,12 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
-# k_accumulate<Fp> at G1 2^20, from the ncu capture summarised in
+# k_accumulate<Fp> at G1 2^20, from the ncu captures summarised in
 # profiles/k_accumulate_g1_2p20.md: DRAM bytes per launch and pipe utilisation
-ACC_TRAFFIC_NCU = 1.586e9
-ACC_PIPES_NCU = {"fp64": 0.476, "alu": 0.545, "fma": 0.072, "issue": 0.589}
+# of the default (integer-product) kernel and of the FP64-product mode
+ACC_TRAFFIC_NCU = 1.592e9
+ACC_PIPES_NCU = {"fmaheavy_imad": 0.870, "alu": 0.219, "issue": 0.410}
+ACC_PIPES_NCU_FP64 = {"fp64": 0.476, "alu": 0.545, "fma": 0.072, "issue": 0.589}
 
 # CPU baseline: reference host code (or the oracle port) on a bounded sample
 # ---------------------------------------------------------------------------
@@ -368,8 +370,8 @@ def run_ours(args, rank, world, local_rank):
     # roofline denominator: the IMAD issue peak (mad.lo only), against which
     # the fixed op count (798 IMAD-equivalents per Fp product) is quoted.  The
     # lo/hi mix of an integer Montgomery product runs well below it (the hi
-    # halves take extra pipe time); the G1 products run on the FP64 pipe
-    # instead (field_f64.cuh), which is how the kernel gets past that mix.
+    # halves take extra pipe time); the optional FP64-product mode
+    # (extra.g1_fp64_products) computes the same products on the FP64 pipe.
     imad_peak = peaks[1]
 
     acc_ms = phase_ms.get("accumulate", float("nan"))
@@ -395,7 +397,7 @@ def run_ours(args, rank, world, local_rank):
                      "peak_source": "measured: gm_imad_probe mode 1 (independent mad.lo chains over all SMs)",
                      "peak_lo_hi_mix": peaks[0] / 1e12,
                      "fp64_fma_peak": peaks[2] / 1e12,
-                     "products_on": "FP64 pipe (DFMA.RZ exact splits, int64 column sums)",
+                     "products_on": "IMAD pipe (CIOS, mad.lo.cc/madc.hi.cc)",
                      "pipes_busy_ncu": ACC_PIPES_NCU},
         "msm_roofline": {"ops_imad": msm_ops, "achieved": msm_ops / (ms / 1e3) / 1e12,
                          "frac": msm_ops / (ms / 1e3) / imad_peak, "unit": "TIMAD/s"},
@@ -408,6 +410,8 @@ def run_ours(args, rank, world, local_rank):
         line["e2e"] = measure_e2e(args, gm, sc, pts_d)
         if not args.no_extra:
             line["extra"] = measure_extra(gm, wl, dev, imad_peak)
+            line["extra"]["g1_fp64_products"] = measure_fp64_mode(gm, pts_d, sc_d, entries, imad_peak,
+                                                                   max(3, args.steps // 2))
             pts_h = gm.to_numpy_points(pts_d[:CPU_SAMPLE], 1)
             v, kind, dt = cpu_baseline_run(pts_h, sc[:CPU_SAMPLE], host_threads())
             line["cpu_baseline"] = {
@@ -466,6 +470,44 @@ def measure_e2e(args, gm, sc, pts_d):
             "api": "gm_g1_msm_host_async on 2 streams (host buffers, pinned)", "results_equal": ok,
             "sync_value": n / sync_dt, "sync_ms_per_step": sync_dt * 1e3,
             "sync_api": "g1_msm_limbs_wrapper (host buffers, pinned)"}
+
+
+def measure_fp64_mode(gm, pts_d, sc_d, entries, imad_peak, steps):
+    """G1 2^20 with the accumulation's products on the FP64 pipe
+    (gm_set_fp64_products): the same MSM, bit-identical result."""
+    import torch
+    n = pts_d.shape[0]
+    out = torch.empty(gm.G1P_WORDS, dtype=torch.int64, device=pts_d.device)
+    ref = torch.empty_like(out)
+    gm.msm_device(pts_d, sc_d, group=1, out=ref)
+    gm.set_fp64_products(True)
+    try:
+        for _ in range(2):
+            gm.msm_device(pts_d, sc_d, group=1, out=out)
+        torch.cuda.synchronize()
+        gm.profile_enable(True)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            gm.msm_device(pts_d, sc_d, group=1, out=out)
+        e1.record()
+        torch.cuda.synchronize()
+        acc = {}
+        for k, v in gm.profile_collect():
+            if k != "start":
+                acc.setdefault(k, []).append(v)
+        gm.profile_enable(False)
+    finally:
+        gm.set_fp64_products(False)
+    ms = e0.elapsed_time(e1) / steps
+    phases = {k: statistics.mean(v) for k, v in acc.items()}
+    same = np.array_equal(gm.canonical_affine(gm.to_numpy_proj(out, 1), 1),
+                          gm.canonical_affine(gm.to_numpy_proj(ref, 1), 1))
+    acc_ms = phases.get("accumulate", float("nan"))
+    return {"points_per_s": n / (ms / 1e3), "ms": ms, "phases_ms": phases, "result_equal_to_default": same,
+            "accumulate_imad_frac": 798.0 * 10 * entries / (acc_ms / 1e3) / imad_peak,
+            "pipes_busy_ncu": ACC_PIPES_NCU_FP64,
+            "products_on": "FP64 pipe (fma.rz.f64 exact splits of 52-bit limbs, int64 column sums)"}
 
 
 def measure_extra(gm, wl, dev, imad_peak):

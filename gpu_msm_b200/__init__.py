@@ -66,6 +66,7 @@ C_API = [
     "gm_batch_run", "gm_batch_workspace_bytes", "gm_g1_sum_projective_host",
     "gm_host_selftest", "gm_fp_elem", "gm_fp2_elem", "gm_g1_point_elem", "gm_g2_point_elem",
     "gm_g1_on_curve_batch", "gm_g2_on_curve_batch", "gm_g1_msm_host_async", "gm_g2_msm_host_async",
+    "gm_set_fp64_products", "gm_fp64_products",
 ]
 
 
@@ -138,6 +139,7 @@ def lib() -> ctypes.CDLL:
             getattr(L, name).argtypes = [vp, u32, vp, i64, vp]
         for name in ("gm_g1_msm_host_async", "gm_g2_msm_host_async"):
             getattr(L, name).argtypes = [vp, u32, vp, vp, vp, i32, i32, i32, vp]
+        L.gm_set_fp64_products.argtypes = [i32]
         _lib = L
     return _lib
 
@@ -561,6 +563,18 @@ def to_numpy_proj(t, group: int = 1) -> np.ndarray:
 # ---------------------------------------------------------------------------
 # measurement hooks
 # ---------------------------------------------------------------------------
+
+def set_fp64_products(on: bool = True):
+    """Product mode of the G1 bucket accumulation: False (default) = the
+    integer CIOS product on the IMAD pipe; True = the bit-identical product on
+    the FP64 pipe (exact 52-bit splits by fma.rz.f64, faster on B200).  Read
+    when an MSM or a batch plan is launched or created."""
+    lib().gm_set_fp64_products(1 if on else 0)
+
+
+def fp64_products() -> bool:
+    return bool(lib().gm_fp64_products())
+
 
 def profile_enable(on: bool = True):
     lib().gm_profile_enable(1 if on else 0)

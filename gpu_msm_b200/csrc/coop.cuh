@@ -15,10 +15,11 @@ namespace gm {
 // Cooperative point operations per group (quads for both groups).
 template <class F>
 struct Coop;
-// G1 quads on FP64-pipe products: the G1 2^20 reduction measured 1.85 ms
-// against 1.91 ms with integer products in the quads.
+// Build switch: G1 quads on FP64-pipe products (field_f64.cuh).  Off by
+// default; on (with GM_OOL_F64), the G1 2^20 reduction measured 1.85 ms
+// against 2.03 ms.
 #ifndef GM_COOP_F64
-#define GM_COOP_F64 1
+#define GM_COOP_F64 0
 #endif
 template <>
 struct Coop<Fp> {

@@ -176,14 +176,6 @@ static __device__ __noinline__ fp_t fp_mul_f64_call(fp_t a, fp_t b) {
   f64::mont_mul(r.v, a.v, b.v);
   return r;
 }
-// Fp with the FP64 product inline (element-wise kernels with one call site)
-struct FpF64 : Fp {
-  GM_DEVI static fp_t mul(const fp_t &a, const fp_t &b) {
-    fp_t r;
-    f64::mont_mul(r.v, a.v, b.v);
-    return r;
-  }
-};
 // The accumulation-loop policy with the FP64 product (squares through it too)
 struct FpOutF64 : Fp {
   GM_DEVI static fp_t mul(const fp_t &a, const fp_t &b) { return fp_mul_f64_call(a, b); }

@@ -5,9 +5,8 @@
 //
 // One element per thread in a grid-stride loop over a grid sized to the SM
 // count; elements are 56 B (Fp) / 112 B (Fp2) records read and written as
-// u64 words, so a warp touches contiguous memory.  The kernels are
-// compute-bound: one Fp product (798 IMAD-equivalents, here on the FP64 pipe)
-// against 168 B of traffic.
+// u64 words, so a warp touches contiguous memory.  The kernels are IMAD-bound:
+// 798 IMAD per Fp product against 168 B of traffic.
 #include <cuda_runtime.h>
 
 #include <type_traits>
@@ -24,9 +23,7 @@ template <class F, int OP>
 __global__ void __launch_bounds__(256) k_field_mul(uint64_t *__restrict__ c, const uint64_t *__restrict__ a,
                                                    const uint64_t *__restrict__ b, int64_t n) {
   constexpr int Hw = F::LIMBS / 2;
-  // Fp products run on the FP64 pipe (field_f64.cuh: the same function as
-  // the integer CIOS product; 2^26 products at 20-22 G/s against 17.9 G/s)
-  using M = typename std::conditional<F::LIMBS == gm::NL, gm::FpF64, F>::type;
+  using M = F;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     typename F::T x, y;
     gm::load_ref<F>(x, a + i * Hw);
@@ -150,6 +147,13 @@ int gm_profile_collect(char *names, int names_len, float *ms, int max) {
 }
 
 int64_t gm_launch_count_reset(void) { return gm::launches_and_reset(); }
+
+int gm_set_fp64_products(int on) {
+  gm::set_fp64_products(on != 0);
+  return gm::GM_OK;
+}
+
+int gm_fp64_products(void) { return gm::fp64_products() ? 1 : 0; }
 
 
 int gm_fp_mont_mul_array(gm_stream_t stream, uint32_t gpu_index, Fp *d_c, const Fp *d_a, const Fp *d_b, int64_t n) {

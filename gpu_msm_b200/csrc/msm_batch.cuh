@@ -22,6 +22,7 @@ struct BatchClassPlan {
   int count = 0;        // MSMs in this class
   int64_t P = 0;        // points in this class
   int64_t K = 0, nb = 0, nthreads = 0;
+  bool fp64 = false;    // accumulation product mode, fixed when the plan is made
   RedLayout rl;
   int64_t long_cap = 0;
   // fixed-base window table (precomputed mode): record w*pc_stride + base
@@ -57,7 +58,8 @@ void batch_class_layout(BatchClassPlan &cp, int limbs, int sms, int dev) {
   const int64_t groups = (int64_t)cp.count * (cp.pc_stride ? 1 : cp.dp.W);
   cp.K = groups * cp.dp.B;
   cp.nb = (cp.K + SCAN_TILE - 1) / SCAN_TILE;
-  cp.nthreads = (int64_t)sms * acc_blocks_per_sm<F>(dev) * ACC_THREADS;
+  cp.fp64 = acc_fp64<F>();
+  cp.nthreads = (int64_t)sms * acc_blocks_per_sm<F>(dev, cp.fp64) * ACC_THREADS;
   const int64_t max_entries = cp.P * cp.dp.W;
   if (cp.nthreads > max_entries) cp.nthreads = std::max<int64_t>(1, (max_entries + 127) / 128 * 128);
   Carve cv;
@@ -117,8 +119,8 @@ int batch_class_run(const BatchPlan &plan, const BatchClassPlan &cp, cudaStream_
                                                       entries);
   GM_CHECK_LAUNCH("k_scatter_multi");
   launches += 5;
-  k_accumulate<F><<<grid_for(cp.nthreads, ACC_THREADS), ACC_THREADS, acc_smem_bytes<F>(), s>>>(
-      cp.pc_table ? cp.pc_table : plan.bases, entries, offsets, cp.K, cp.nthreads, buckets, head, tail, hk, tk);
+  acc_launch<F>(cp.fp64, grid_for(cp.nthreads, ACC_THREADS), s, cp.pc_table ? cp.pc_table : plan.bases, entries,
+                offsets, cp.K, cp.nthreads, buckets, head, tail, hk, tk);
   GM_CHECK_LAUNCH("k_accumulate");
   launches++;
   int rc = fixup_launch<F>(s, offsets, cp.K, cp.nthreads, buckets, head, tail, hk, tk, err, long_q, cp.long_cap,

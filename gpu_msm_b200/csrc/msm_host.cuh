@@ -108,23 +108,86 @@ struct MsmLayout {
   }
 };
 
-// Blocks of k_accumulate resident per SM; the dynamic shared-memory opt-in is
-// a per-device function attribute, so it is set (and cached) per device.
-template <class F>
-static int acc_blocks_per_sm(int dev) {
+// k_accumulate runs at most ACC_BLOCKS_MAX blocks per SM.  Its slices carry
+// equal work, so a block that shares its SM with more blocks than the others
+// finishes late and holds up the whole launch: with 3 blocks per SM the G1
+// 2^20 accumulation took 13.8 ms against 13.3 ms, and batches, whose classes'
+// launches overlap, 196 ms against 143 ms.  The grid holds ACC_BLOCKS_MAX
+// blocks per SM, and where the registers would let more blocks share an SM
+// the launch asks for enough dynamic shared memory to keep them out.
+constexpr int ACC_BLOCKS_MAX = 2;
+
+struct AccOccupancy {
+  int blocks = 0;     // resident blocks per SM the grid is sized for
+  size_t smem = 0;    // dynamic shared memory of a launch
+};
+
+template <class F, bool FP64>
+static AccOccupancy acc_occupancy(int dev) {
   static std::mutex mu;
-  static int cached[64] = {0};
+  static AccOccupancy cached[64];
   std::lock_guard<std::mutex> lk(mu);
   if (dev < 0 || dev >= 64) dev = 0;
-  if (cached[dev] == 0) {
-    int b = 0;
-    cudaFuncSetAttribute(k_accumulate<F>, cudaFuncAttributeMaxDynamicSharedMemorySize, acc_smem_bytes<F>());
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_accumulate<F>, ACC_THREADS, acc_smem_bytes<F>()) !=
-        cudaSuccess)
+  AccOccupancy &o = cached[dev];
+  if (o.blocks == 0) {
+    size_t smem = acc_smem_bytes<F>();
+    int per_sm_smem = 0, b = 0;
+    cudaDeviceGetAttribute(&per_sm_smem, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    cudaFuncSetAttribute(k_accumulate<F, FP64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_accumulate<F, FP64>, ACC_THREADS, smem) != cudaSuccess)
       b = 1;
-    cached[dev] = std::max(1, b);
+    if (b > ACC_BLOCKS_MAX && per_sm_smem > 0) {
+      // (ACC_BLOCKS_MAX + 1) blocks must not fit in the SM's shared memory
+      const size_t pad = (size_t)per_sm_smem / (ACC_BLOCKS_MAX + 1) + 1024;
+      if (cudaFuncSetAttribute(k_accumulate<F, FP64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pad) ==
+          cudaSuccess)
+        smem = pad;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_accumulate<F, FP64>, ACC_THREADS, smem) !=
+          cudaSuccess)
+        b = 1;
+    }
+    o.smem = smem;
+    o.blocks = std::max(1, std::min(b, ACC_BLOCKS_MAX));
   }
-  return cached[dev];
+  return o;
+}
+
+template <class F, bool FP64>
+static int acc_blocks_per_sm_mode(int dev) {
+  return acc_occupancy<F, FP64>(dev).blocks;
+}
+
+// Whether the accumulation of group F uses FP64-pipe products (G1 only, when
+// the run-time mode is on).
+template <class F>
+static bool acc_fp64() {
+  return F::LIMBS == NL && fp64_products();
+}
+
+template <class F>
+static int acc_blocks_per_sm(int dev, bool fp64) {
+  if constexpr (F::LIMBS == NL) {
+    if (fp64) return acc_blocks_per_sm_mode<F, true>(dev);
+  }
+  return acc_blocks_per_sm_mode<F, false>(dev);
+}
+
+// k_accumulate in the chosen product mode
+template <class F>
+static void acc_launch(bool fp64, unsigned grid, cudaStream_t s, const uint4 *bases, const uint32_t *entries,
+                       const uint32_t *offsets, int64_t K, int64_t nthreads, xyzz_t<F> *buckets, xyzz_t<F> *head,
+                       xyzz_t<F> *tail, int32_t *hk, int32_t *tk) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if constexpr (F::LIMBS == NL) {
+    if (fp64) {
+      k_accumulate<F, true><<<grid, ACC_THREADS, acc_occupancy<F, true>(dev).smem, s>>>(
+          bases, entries, offsets, K, nthreads, buckets, head, tail, hk, tk);
+      return;
+    }
+  }
+  k_accumulate<F, false><<<grid, ACC_THREADS, acc_occupancy<F, false>(dev).smem, s>>>(
+      bases, entries, offsets, K, nthreads, buckets, head, tail, hk, tk);
 }
 
 static inline unsigned grid_for(int64_t n, int block) { return (unsigned)((n + block - 1) / block); }
@@ -221,7 +284,8 @@ int msm_launch(cudaStream_t s, int dev, const uint4 *bases, const uint64_t *ref_
     return GM_ERR_ARG;
   }
   MsmLayout<F> lay;
-  lay.plan(n, limbs, c, sms, acc_blocks_per_sm<F>(dev), bases == nullptr, /*leveled=*/true,
+  const bool fp64 = acc_fp64<F>();
+  lay.plan(n, limbs, c, sms, acc_blocks_per_sm<F>(dev, fp64), bases == nullptr, /*leveled=*/true,
            (int64_t)sms * level0_blocks_per_sm<F>(dev) * 128);
   lay.rl.dev = dev;
   if ((uint64_t)n * lay.dp.W >= (1ull << 32)) {
@@ -269,8 +333,8 @@ int msm_launch(cudaStream_t s, int dev, const uint4 *bases, const uint64_t *ref_
     launches++;
     profile_mark(s, "pack");
   }
-  k_accumulate<F><<<grid_for(lay.nthreads, ACC_THREADS), ACC_THREADS, acc_smem_bytes<F>(), s>>>(bases, entries, offsets, lay.K, lay.nthreads, buckets,
-                                                               head, tail, hk, tk);
+  acc_launch<F>(fp64, grid_for(lay.nthreads, ACC_THREADS), s, bases, entries, offsets, lay.K, lay.nthreads, buckets,
+                head, tail, hk, tk);
   GM_CHECK_LAUNCH("k_accumulate");
   launches++;
   profile_mark(s, "accumulate");

@@ -48,10 +48,11 @@ struct Rec<Fp2> {
 // Arithmetic policy with the field product out of line (same data types).
 template <class F>
 struct OutOfLine;
-// Fp products on the FP64 pipe (field_f64.cuh) outside the accumulation
-// too: the G1 reduction of 2^20 points measured 1.91 ms against 2.03 ms.
+// Build switch: Fp products of the reduction kernels on the FP64 pipe
+// (field_f64.cuh).  Off by default -- the path stays on integer instructions;
+// on, the G1 2^20 reduction measured 1.91 ms against 2.03 ms.
 #ifndef GM_OOL_F64
-#define GM_OOL_F64 1
+#define GM_OOL_F64 0
 #endif
 template <>
 struct OutOfLine<Fp> {
@@ -71,23 +72,20 @@ struct OutOfLine<Fp2> {
 // Policy of the accumulation loop (one out-of-line product only).
 template <class F>
 struct AccPolicy;
-// G1: the Montgomery product on the FP64 pipe (field_f64.cuh), bit-identical
-// to the integer one.  The integer product is bound by IMAD.HI issue on the
-// FMA pipe; measured on B200 for the G1 2^20 accumulation: 11.25 ms against
-// 13.28 ms.  (The same swap inside the G2 Fp2 product measured 12.21 ms
-// against 12.02 ms for G2 2^18, so G2 keeps the integer product.)
+// G1 accumulation product: the integer CIOS product by default.  The
+// FP64-pipe product (field_f64.cuh, bit-identical) is chosen at run time
+// instead when set_fp64_products(true) -- see AccSel below; GM_ACC_F64 sets
+// that mode's initial value.  Measured on B200 for the G1 2^20 accumulation:
+// 11.10 ms with FP64-pipe products against 13.28 ms.  (Inside the G2 Fp2
+// product it measured 12.21 ms against 12.02 ms, so G2 has no FP64 mode.)
 #ifndef GM_ACC_F64
-#define GM_ACC_F64 1
+#define GM_ACC_F64 0
 #endif
 // One product function only: squares on the integer pipe beside FP64-pipe
 // products (two out-of-line functions in the loop) measured 15.12 ms.
 template <>
 struct AccPolicy<Fp> {
-#if GM_ACC_F64
-  using type = FpOutF64;
-#else
   using type = FpOutMulOnly;
-#endif
 };
 // G2: the whole Fp2 product out of line.  Inlined Karatsuba sums around 30
 // Fp calls made the loop overflow the instruction cache (ncu: 9.9% of warp
@@ -96,6 +94,17 @@ struct AccPolicy<Fp> {
 template <>
 struct AccPolicy<Fp2> {
   using type = Fp2Call;
+};
+
+// Accumulation policy for the run-time product mode: FP64-pipe products for
+// G1 when FP64 is set, else AccPolicy's.
+template <class F, bool FP64>
+struct AccSel {
+  using type = typename AccPolicy<F>::type;
+};
+template <>
+struct AccSel<Fp, true> {
+  using type = FpOutF64;
 };
 
 template <class A, class B>
@@ -549,17 +558,14 @@ struct StagedPoint {
 // laid out chunk-major ([slot][chunk][thread]) so a warp's 16-byte accesses
 // hit consecutive banks.  Only the owning thread reads its slots, so no
 // block-level barrier is needed.
-template <class F>
-#ifndef GM_ACC_MIN_BLOCKS
-#define GM_ACC_MIN_BLOCKS 1
-#endif
-__global__ void __launch_bounds__(ACC_THREADS, GM_ACC_MIN_BLOCKS) k_accumulate(const uint4 *__restrict__ bases, const uint32_t *__restrict__ entries,
+template <class F, bool FP64 = false>
+__global__ void __launch_bounds__(ACC_THREADS) k_accumulate(const uint4 *__restrict__ bases, const uint32_t *__restrict__ entries,
                                                     const uint32_t *__restrict__ offsets, int64_t K, int64_t nthreads,
                                                     xyzz_t<F> *__restrict__ buckets,
                                                     xyzz_t<F> *__restrict__ part_head, xyzz_t<F> *__restrict__ part_tail,
                                                     int32_t *__restrict__ head_key, int32_t *__restrict__ tail_key) {
   using T = typename F::T;
-  using FA = typename AccPolicy<F>::type;
+  using FA = typename AccSel<F, FP64>::type;
   constexpr int CH = F::LIMBS / 2;  // 16-byte chunks of x || y
   extern __shared__ uint4 stage_mem[];  // [2][CH][ACC_THREADS], acc_smem_bytes<F>()
   auto stage = reinterpret_cast<uint4(*)[CH][ACC_THREADS]>(stage_mem);

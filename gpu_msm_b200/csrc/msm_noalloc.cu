@@ -99,7 +99,7 @@ extern "C" int gm_g1_msm_device_noalloc(gm_stream_t stream, uint32_t gpu_index, 
     return gm::GM_ERR_ARG;
   }
   // sets the accumulation kernel's dynamic shared-memory attribute (no allocation)
-  (void)gm::acc_blocks_per_sm<Fp>((int)gpu_index);
+  (void)gm::acc_blocks_per_sm<Fp>((int)gpu_index, false);
 
   char *ws = static_cast<char *>(base);
   auto *counts = (uint32_t *)(ws + lay.o_counts);

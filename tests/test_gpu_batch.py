@@ -203,3 +203,21 @@ def test_batch_precomputed_g2(cuda):
     res = gm.BatchPlan(table, sizes, offs).run(t_dev(sc, cuda).reshape(-1, 5))
     torch.cuda.synchronize()
     check(res, expected(sizes, offs, sc, logs, 2), 2)
+
+
+def test_batch_fp64_products_mode(cuda):
+    """Batch plans made in the FP64-product mode (G1 accumulation products on
+    the FP64 pipe), with and without window tables, equal the oracle."""
+    import torch
+    gm.set_fp64_products(True)
+    try:
+        table, logs = make_table(1 << 11, 1, cuda, seed=171)
+        table.precompute(8)
+        sizes, offs, sc = batch_inputs(1 << 11, 24, 1, 11, seed=172)
+        wins = np.array([[5, 8][i % 2] for i in range(len(sizes))], dtype=np.int32)
+        plan = gm.BatchPlan(table, sizes, offs, window_bits=wins)
+        res = plan.run(t_dev(sc, cuda).reshape(-1, 5))
+        torch.cuda.synchronize()
+        check(res, expected(sizes, offs, sc, logs, 1), 1)
+    finally:
+        gm.set_fp64_products(False)

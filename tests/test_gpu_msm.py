@@ -352,3 +352,41 @@ def test_max_size_exact_relation(cuda, group, n):
     s = gm.sum_projective(both, group=group)
     torch.cuda.synchronize()
     assert oracle.same_point(oracle.proj_to_affine(gm.to_numpy_proj(s, group), group), want)
+
+
+@pytest.fixture
+def fp64_products():
+    """The FP64-pipe product mode of the G1 accumulation, for one test."""
+    gm.set_fp64_products(True)
+    assert gm.fp64_products()
+    yield
+    gm.set_fp64_products(False)
+
+
+@pytest.mark.parametrize("n,c", [(1, 0), (100, 0), (4097, 0), (1 << 16, 0), (3000, 3), (20000, 13)])
+def test_fp64_products_mode(cuda, fp64_products, n, c):
+    """gm_set_fp64_products(1): the G1 accumulation's Montgomery products on
+    the FP64 pipe give the exact result, for ragged sizes, small and large
+    windows and heavy buckets (most scalars 1 or 2)."""
+    sc = wl.make_scalars(n, seed=3100 + n + c)
+    if c == 3:
+        sc[: n * 2 // 3] = 0
+        sc[: n // 3, 0] = 1
+        sc[n // 3: n * 2 // 3, 0] = 2
+    logs = wl.make_base_logs(n, seed=3200 + n + c)
+    pts = make_bases(logs, 1, cuda)
+    want = oracle.generator_multiple(wl.expected_log(sc, logs))
+    assert oracle.same_point(device_msm(pts, sc, 1, cuda, c=c), want)
+
+
+def test_fp64_products_mode_full_size(cuda, fp64_products):
+    """The bench workload in the FP64-product mode: the exact relation at
+    2^20 and the same canonical point as the default (integer) mode."""
+    n = 1 << 20
+    sc = wl.make_scalars(n, seed=42)
+    logs = wl.make_base_logs(n, seed=4242)
+    pts = make_bases(logs, 1, cuda)
+    got = device_msm(pts, sc, 1, cuda)
+    assert oracle.same_point(got, oracle.generator_multiple(wl.expected_log(sc, logs)))
+    gm.set_fp64_products(False)
+    assert oracle.same_point(device_msm(pts, sc, 1, cuda), got)
