@@ -180,8 +180,8 @@ class ClockSampler:
 # k_accumulate<Fp> at G1 2^20, from the ncu captures summarised in
 # profiles/k_accumulate_g1_2p20.md: DRAM bytes per launch and pipe utilisation
 # of the default (integer-product) kernel and of the FP64-product mode
-ACC_TRAFFIC_NCU = 1.592e9
-ACC_PIPES_NCU = {"fmaheavy_imad": 0.870, "alu": 0.219, "issue": 0.410}
+ACC_TRAFFIC_NCU = 1.594e9
+ACC_PIPES_NCU = {"fmaheavy_imad": 0.875, "alu": 0.215, "issue": 0.408}
 ACC_PIPES_NCU_FP64 = {"fp64": 0.476, "alu": 0.545, "fma": 0.072, "issue": 0.589}
 
 # CPU baseline: reference host code (or the oracle port) on a bounded sample
