@@ -13,6 +13,9 @@ Keys beyond the driver contract:
                 this GPU (bound "imad": the path is exact integer arithmetic;
                 neither tensor cores nor HBM bound it)
   msm_roofline  the whole MSM against the same peak, with the fixed op count
+  value         timed steps run round-robin over PIPELINE_STREAMS streams
+                (consecutive MSMs overlap); ms_per_step_serial is one stream,
+                and the phase times and roofline come from that serial pass
   cpu_baseline  the reference's own host code (oracle/_ref) on the host cores
   extra         Fp 2^26 and G2 2^18 measurements, phase breakdown, the
                 optional FP64-product mode of the G1 accumulation
@@ -38,6 +41,10 @@ sys.path.insert(0, ROOT)
 
 LOG2N = 20
 G2_LOG2N = 18
+# the timed plain-MSM steps run round-robin over this many streams: one MSM's
+# latency-bound tail (upper reduction levels, host window combine) then
+# overlaps the next MSM's accumulation (G1 2^20: 16.6 -> 15.3 ms per MSM)
+PIPELINE_STREAMS = 3
 CPU_SAMPLE = 1 << 14
 FP_MICRO = 1 << 26
 METRIC = "MSM points/s (G1 2^20, G2 2^18) batched vs plain on 1 B200, bit-exact; p99 ms"
@@ -300,43 +307,81 @@ def run_ours(args, rank, world, local_rank):
     c = gm.default_window(1, n, 5)
     entries = int(wl.signed_digit_counts(sc, c).sum())
 
-    gathered = torch.empty((world, gm.G1P_WORDS), dtype=torch.int64, device=dev) if world > 1 else None
+    # one result (and gather) buffer per stream, so that MSMs in flight on
+    # different streams never share one
+    outs = [torch.empty(gm.G1P_WORDS, dtype=torch.int64, device=dev) for _ in range(PIPELINE_STREAMS)]
+    gathered = [torch.empty((world, gm.G1P_WORDS), dtype=torch.int64, device=dev) if world > 1 else None
+                for _ in range(PIPELINE_STREAMS)]
 
-    def step(out):
-        gm.msm_device(pts_d, sc_d, group=1, out=out)
+    def step(k, stream):
+        with torch.cuda.stream(stream):
+            gm.msm_device(pts_d, sc_d, group=1, out=outs[k], stream=stream)
+            if world > 1:
+                dist.all_gather_into_tensor(gathered[k], outs[k])
+                gm.sum_projective(gathered[k], group=1, out=outs[k], stream=stream)
+
+    main = torch.cuda.current_stream()
+    side = [torch.cuda.Stream() for _ in range(PIPELINE_STREAMS)]
+
+    def run_steps(steps, pipelined):
+        """Device time per step (ms): one stream, or steps round-robin over
+        PIPELINE_STREAMS streams (one step's latency-bound tail -- upper
+        reduction levels, host combine -- overlaps the next step's
+        accumulation)."""
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(main)
+        if pipelined:
+            for s in side:
+                s.wait_stream(main)
+            for i in range(steps):
+                step(i % PIPELINE_STREAMS, side[i % PIPELINE_STREAMS])
+            for s in side:
+                main.wait_stream(s)
+        else:
+            for _ in range(steps):
+                step(0, main)
+        ev1.record(main)
+        torch.cuda.synchronize()
+        return ev0.elapsed_time(ev1) / steps
+
+    def max_over_ranks(ms):
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
         if world > 1:
-            dist.all_gather_into_tensor(gathered, out)
-            gm.sum_projective(gathered, group=1, out=out)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
 
-    out = torch.empty(gm.G1P_WORDS, dtype=torch.int64, device=dev)
     for _ in range(args.warmup):
-        step(out)
+        step(0, main)
     torch.cuda.synchronize()
 
-    # timed region: device events on the launching (current) stream
-    gm.launch_count_reset()
+    # serial pass (one stream, phase events on): the per-phase times and the
+    # dominant kernel's duration for the roofline, free of other MSMs' kernels
     gm.profile_enable(True)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ms = run_steps(args.steps, pipelined=False)
+    phases = gm.profile_collect()
+    gm.profile_enable(False)
+    serial_ms_max = max_over_ranks(ms)
+    serial_aff = gm.canonical_affine(gm.to_numpy_proj(outs[0], 1), 1)
+
+    # timed region: the same steps, pipelined over PIPELINE_STREAMS streams
+    run_steps(max(args.warmup, PIPELINE_STREAMS), pipelined=True)
+    gm.launch_count_reset()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
     with ClockSampler(local_rank) as clk:
-        ev0.record()
-        for _ in range(args.steps):
-            step(out)
-        ev1.record()
-        torch.cuda.synchronize()
+        ms_pipe = run_steps(args.steps, pipelined=True)
     if world > 1:
         dist.barrier()
     launches = gm.launch_count_reset()
-    phases = gm.profile_collect()
-    gm.profile_enable(False)
-    ms = ev0.elapsed_time(ev1) / args.steps
-    t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = max_over_ranks(ms_pipe)
     value = world * n / (ms_max / 1e3)
+    # every pipelined step's result equals the serial one (compared in affine
+    # form: projective coordinates depend on the order of additions in a bucket)
+    pipelined_ok = all(np.array_equal(gm.canonical_affine(gm.to_numpy_proj(o, 1), 1), serial_aff) for o in outs)
 
     # per-phase averages and the dominant kernel
     acc = {}
@@ -386,7 +431,10 @@ def run_ours(args, rank, world, local_rank):
         "config": {"workload": f"plain single G1 MSM, n=2^{LOG2N} per GPU, scalars < r (5 x u64), "
                                "1% zeros, 1% ones, bases t_i*G with 2% duplicates",
                    "window_bits": c, "entries": entries, "parallelism": f"points sharded x{world}",
+                   "streams": f"{PIPELINE_STREAMS} (consecutive steps round-robin; each step a full MSM)",
                    "l2": "inputs 168 MB > 126 MB L2 (no flush)"},
+        "ms_per_step_serial": serial_ms_max,
+        "pipelined_results_equal": bool(pipelined_ok),
         "roofline": {"bound": "imad", "kernel": "k_accumulate<Fp>", "achieved": achieved / 1e12,
                      "peak": imad_peak / 1e12, "unit": "TIMAD/s", "frac": achieved / imad_peak,
                      # dram__bytes_read + dram__bytes_write of one launch, from the ncu
@@ -399,8 +447,9 @@ def run_ours(args, rank, world, local_rank):
                      "fp64_fma_peak": peaks[2] / 1e12,
                      "products_on": "IMAD pipe (CIOS, mad.lo.cc/madc.hi.cc)",
                      "pipes_busy_ncu": ACC_PIPES_NCU},
-        "msm_roofline": {"ops_imad": msm_ops, "achieved": msm_ops / (ms / 1e3) / 1e12,
-                         "frac": msm_ops / (ms / 1e3) / imad_peak, "unit": "TIMAD/s"},
+        "msm_roofline": {"ops_imad": msm_ops, "achieved": msm_ops / (ms_max / 1e3) / 1e12,
+                         "frac": msm_ops / (ms_max / 1e3) / imad_peak, "unit": "TIMAD/s",
+                         "frac_serial": msm_ops / (serial_ms_max / 1e3) / imad_peak},
         "phases_ms": phase_ms,
         "gpu_launches": int(launches),
     }
@@ -426,9 +475,9 @@ def measure_e2e(args, gm, sc, pts_d):
     every step copies its points and scalars to the device, runs the MSM and
     reads its result back to the host.
 
-    value: gm_g1_msm_host_async on two streams, so that one step's copies
-    overlap the previous step's compute (each step's copies and result read
-    are still inside the timed region).  sync_value: the blocking
+    value: gm_g1_msm_host_async round-robin on PIPELINE_STREAMS streams, so
+    that one step's copies overlap the previous steps' compute (each step's
+    copies and result read are still inside the timed region).  sync_value: the blocking
     g1_msm_limbs_wrapper, one MSM at a time."""
     import torch
     n = len(sc)
@@ -447,27 +496,28 @@ def measure_e2e(args, gm, sc, pts_d):
         gm.msm(pts_np, sc_np, group=1, montgomery=True)
     sync_dt = (time.perf_counter() - t0) / steps
 
-    streams = [torch.cuda.Stream(), torch.cuda.Stream()]
-    res_pin = torch.zeros((steps + 2, gm.G1P_WORDS), dtype=torch.int64, pin_memory=True)
+    ns = PIPELINE_STREAMS
+    streams = [torch.cuda.Stream() for _ in range(ns)]
+    res_pin = torch.zeros((steps + ns, gm.G1P_WORDS), dtype=torch.int64, pin_memory=True)
     res_np = res_pin.numpy().view(np.uint64).view(gm.G1P).reshape(-1)
-    err_pin = torch.ones(steps + 2, dtype=torch.int32, pin_memory=True)
+    err_pin = torch.ones(steps + ns, dtype=torch.int32, pin_memory=True)
     err_np = err_pin.numpy().view(np.uint32)
-    for i in range(2):
+    for i in range(ns):
         gm.msm_host_async(pts_np, sc_np, res_np[i:i + 1], stream=streams[i], err=err_np[i:i + 1])
     for st in streams:
         st.synchronize()
     t0 = time.perf_counter()
-    for i in range(2, steps + 2):
-        gm.msm_host_async(pts_np, sc_np, res_np[i:i + 1], stream=streams[i % 2], err=err_np[i:i + 1])
+    for i in range(ns, steps + ns):
+        gm.msm_host_async(pts_np, sc_np, res_np[i:i + 1], stream=streams[i % ns], err=err_np[i:i + 1])
     for st in streams:
         st.synchronize()
     dt = (time.perf_counter() - t0) / steps
     want = gm.canonical_affine(ref.reshape(1), 1)
     ok = bool(err_np.max() == 0) and all(
-        np.array_equal(gm.canonical_affine(res_np[i:i + 1], 1), want) for i in range(steps + 2))
+        np.array_equal(gm.canonical_affine(res_np[i:i + 1], 1), want) for i in range(steps + ns))
     return {"value": n / dt, "unit": "points/s", "h2d_bytes_per_step": n * (120 + 40),
             "d2h_bytes_per_step": 168 + 4, "ms_per_step": dt * 1e3,
-            "api": "gm_g1_msm_host_async on 2 streams (host buffers, pinned)", "results_equal": ok,
+            "api": f"gm_g1_msm_host_async on {ns} streams (host buffers, pinned)", "results_equal": ok,
             "sync_value": n / sync_dt, "sync_ms_per_step": sync_dt * 1e3,
             "sync_api": "g1_msm_limbs_wrapper (host buffers, pinned)"}
 
