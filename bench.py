@@ -607,9 +607,29 @@ def measure_extra(gm, wl, dev, imad_peak):
     for name, v in phases2:
         if name != "start":
             acc2.setdefault(name, []).append(v)
+    # the same MSMs round-robin over PIPELINE_STREAMS streams
+    main = torch.cuda.current_stream()
+    side = [torch.cuda.Stream() for _ in range(PIPELINE_STREAMS)]
+    o2s = [torch.empty(gm.G2P_WORDS, dtype=torch.int64, device=dev) for _ in range(PIPELINE_STREAMS)]
+    preps = 2 * PIPELINE_STREAMS
+    for timed in (False, True):
+        e0.record(main)
+        for st in side:
+            st.wait_stream(main)
+        for i in range(preps):
+            gm.msm_device(pts2, sc2_d, group=2, out=o2s[i % PIPELINE_STREAMS], stream=side[i % PIPELINE_STREAMS])
+        for st in side:
+            main.wait_stream(st)
+        e1.record(main)
+        torch.cuda.synchronize()
+    t2p = e0.elapsed_time(e1) / preps / 1e3
+    want2 = gm.canonical_affine(gm.to_numpy_proj(o2, 2), 2)
+    pipe_ok = all(np.array_equal(gm.canonical_affine(gm.to_numpy_proj(o, 2), 2), want2) for o in o2s)
     out["g2_msm_2^18"] = {"points_per_s": n2 / t2, "ms": t2 * 1e3, "imad_frac": ops2 / t2 / imad_peak,
                           "window_bits": gm.default_window(2, n2, 5),
-                          "phases_ms": {k: statistics.mean(v) for k, v in acc2.items()}}
+                          "phases_ms": {k: statistics.mean(v) for k, v in acc2.items()},
+                          "pipelined": {"streams": PIPELINE_STREAMS, "ms_per_msm": t2p * 1e3,
+                                        "points_per_s": n2 / t2p, "results_equal": bool(pipe_ok)}}
     del pts2, sc2_d
     out["batched_512"] = measure_batched(gm, wl, dev)
     out["serving"] = measure_serving(gm, wl, dev)
