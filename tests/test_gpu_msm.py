@@ -240,6 +240,31 @@ def test_concurrent_streams(cuda):
         assert oracle.same_point(oracle.proj_to_affine(gm.to_numpy_proj(o, 1), 1), w)
 
 
+@pytest.mark.parametrize("group,log2n", [(1, 16), (2, 14)])
+def test_round_robin_streams(cuda, group, log2n):
+    """Consecutive MSMs round-robin over three streams, two per stream (the
+    way bench.py times them): one call's reduction tail and host combine run
+    while the next calls sort and accumulate, each call on its own pool
+    workspace and host-tail slot.  Every result must be its own MSM's."""
+    import torch
+    n = 1 << log2n
+    streams = [torch.cuda.Stream() for _ in range(3)]
+    inputs, wants, outs = [], [], []
+    for i in range(6):
+        sc = wl.make_scalars(n, seed=900 + 10 * group + i)
+        logs = wl.make_base_logs(n, seed=950 + 10 * group + i)
+        inputs.append((make_bases(logs, group, cuda), t_dev(sc, cuda).reshape(n, -1)))
+        wants.append(oracle.generator_multiple(wl.expected_log(sc, logs), group=group))
+    torch.cuda.synchronize()
+    for i, (pts, sc) in enumerate(inputs):
+        s = streams[i % 3]
+        with torch.cuda.stream(s):
+            outs.append(gm.msm_device(pts, sc, group=group, stream=s))
+    torch.cuda.synchronize()
+    for o, w in zip(outs, wants):
+        assert oracle.same_point(oracle.proj_to_affine(gm.to_numpy_proj(o, group), group), w)
+
+
 @pytest.mark.parametrize("group,n,c", [(1, 3000, 0), (1, 3000, 8), (1, 5000, 3), (2, 1000, 0)])
 def test_heavy_buckets(cuda, group, n, c):
     """Most scalars equal to 1 or 2: a few buckets hold thousands of entries
