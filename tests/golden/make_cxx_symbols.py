@@ -84,7 +84,9 @@ void element_calls(cudaStream_t s, uint32_t g, Fp *f, Fp2 *e, G1Point *p1, G2Poi
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: make_cxx_symbols.py <reference checkout>")
+    ref = sys.argv[1]
     out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "cxx_symbols.txt")
     with tempfile.TemporaryDirectory() as d:
         src, obj = os.path.join(d, "refs.cu"), os.path.join(d, "refs.o")
