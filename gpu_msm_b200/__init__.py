@@ -66,7 +66,6 @@ C_API = [
     "gm_batch_run", "gm_batch_workspace_bytes", "gm_g1_sum_projective_host",
     "gm_host_selftest", "gm_fp_elem", "gm_fp2_elem", "gm_g1_point_elem", "gm_g2_point_elem",
     "gm_g1_on_curve_batch", "gm_g2_on_curve_batch", "gm_g1_msm_host_async", "gm_g2_msm_host_async",
-    "gm_set_fp64_products", "gm_fp64_products",
 ]
 
 
@@ -112,7 +111,7 @@ def lib() -> ctypes.CDLL:
         L.gm_profile_collect.argtypes = [ctypes.c_char_p, i32, vp, i32]
         L.gm_launch_count_reset.restype = i64
         L.gm_imad_probe.argtypes = [vp, u32, i32, i32, vp, i64, vp]
-        L.gm_g1_msm_device_noalloc.argtypes = [vp, u32, vp, vp, vp, i32, i32]
+        L.gm_g1_msm_device_noalloc.argtypes = [vp, u32, vp, vp, vp, i32, i32, vp]
         L.gm_bases_create.argtypes = [u32, i32, vp, i64, i32, vp]
         L.gm_bases_destroy.argtypes = [vp]
         L.gm_bases_precompute.argtypes = [vp, i32, i32]
@@ -139,7 +138,6 @@ def lib() -> ctypes.CDLL:
             getattr(L, name).argtypes = [vp, u32, vp, i64, vp]
         for name in ("gm_g1_msm_host_async", "gm_g2_msm_host_async"):
             getattr(L, name).argtypes = [vp, u32, vp, vp, vp, i32, i32, i32, vp]
-        L.gm_set_fp64_products.argtypes = [i32]
         _lib = L
     return _lib
 
@@ -367,11 +365,13 @@ def msm_device_affine(points, scalars, group: int = 1, out=None, stream=None):
 NOALLOC_MAX_POINTS = 4096
 
 
-def msm_device_noalloc(points, scalars, out=None, stream=None):
+def msm_device_noalloc(points, scalars, out=None, err=None, stream=None):
     """G1 MSM through gm_g1_msm_device_noalloc, for callers that cannot
     allocate device memory per call: the workspace is fixed in the library's
     device image, so at most 4096 points per call.  Calls that overlap on the
-    GPU share that workspace and race; keep them on one stream."""
+    GPU share that workspace and race; keep them on one stream.  err: optional
+    int32 CUDA tensor of one element that receives the consistency flag
+    (0 = ok) on the stream."""
     import torch
     _require(points, G1_WORDS, "points")
     n = points.shape[0]
@@ -380,9 +380,11 @@ def msm_device_noalloc(points, scalars, out=None, stream=None):
         out = torch.empty(G1P_WORDS, dtype=torch.int64, device=points.device)
     if out.numel() < G1P_WORDS or out.dtype != torch.int64 or out.device != points.device:
         raise ValueError("out: int64 tensor of the result size on the points' device")
+    if err is not None and (err.dtype != torch.int32 or err.numel() < 1 or err.device != points.device):
+        raise ValueError("err: int32 tensor of one element on the points' device")
     _check(lib().gm_g1_msm_device_noalloc(_stream_handle(stream), _dev_index(points), ctypes.c_void_p(out.data_ptr()),
                                           ctypes.c_void_p(points.data_ptr()), ctypes.c_void_p(scalars.data_ptr()),
-                                          scalars.shape[1], n), "msm_device_noalloc")
+                                          scalars.shape[1], n, _ptr_or_null(err)), "msm_device_noalloc")
     return out
 
 
@@ -564,18 +566,6 @@ def to_numpy_proj(t, group: int = 1) -> np.ndarray:
 # measurement hooks
 # ---------------------------------------------------------------------------
 
-def set_fp64_products(on: bool = True):
-    """Product mode of the G1 bucket accumulation: False (default) = the
-    integer CIOS product on the IMAD pipe; True = the bit-identical product on
-    the FP64 pipe (exact 52-bit splits by fma.rz.f64, faster on B200).  Read
-    when an MSM or a batch plan is launched or created."""
-    lib().gm_set_fp64_products(1 if on else 0)
-
-
-def fp64_products() -> bool:
-    return bool(lib().gm_fp64_products())
-
-
 def profile_enable(on: bool = True):
     lib().gm_profile_enable(1 if on else 0)
 
@@ -596,7 +586,7 @@ def launch_count_reset() -> int:
 
 def imad_probe(iters: int, sink, stream=None, mode: int = 0) -> int:
     """Launch the multiply-add throughput probe (mode 0: mad.lo/mad.hi mix,
-    1: mad.lo only, 2: fma.rn.f64); returns instructions per launch."""
+    1: mad.lo only); returns instructions per launch."""
     import torch
     if not (isinstance(sink, torch.Tensor) and sink.is_cuda and sink.dtype == torch.int32):
         raise ValueError("sink: int32 CUDA tensor")

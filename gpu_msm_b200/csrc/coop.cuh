@@ -1,13 +1,14 @@
 // Cooperative point operations for the latency-bound phases (upper
 // reduction levels, reduction tree, fix-up of long bucket runs, window
 // combination): the lane-group size and the operations per group.  Both
-// groups use quads (xyzz_quad.cuh).  A 16-lane G2 variant (three Karatsuba Fp
-// products of each of the level's four Fp2 products on separate lanes) was
-// measured slower on B200: four times the threads at the same register
-// footprint pushed the upper levels into a second wave (G2 2^18 reduction
-// 5.2 ms against 3.0 ms).
+// groups use quads (xyzz_quad.cuh).  These phases run about one warp per SM
+// sub-partition, and such a warp is bound by its own instruction issue, so
+// wider groups do not help: a G2 variant on 16 lanes with the three
+// Karatsuba Fp products of every Fp2 product on separate lanes issues more
+// instructions per addition (16 lanes x 4 products plus the gathers, against
+// 4 lanes x 12 products) and measured slower on B200 (G2 2^18 level 1
+// 2.46 ms against 1.2 ms on quads).
 #pragma once
-#include "field_f64.cuh"
 #include "xyzz_quad.cuh"
 
 namespace gm {
@@ -15,19 +16,9 @@ namespace gm {
 // Cooperative point operations per group (quads for both groups).
 template <class F>
 struct Coop;
-// Build switch: G1 quads on FP64-pipe products (field_f64.cuh).  Off by
-// default; on (with GM_OOL_F64), the G1 2^20 reduction measured 1.85 ms
-// against 2.03 ms.
-#ifndef GM_COOP_F64
-#define GM_COOP_F64 0
-#endif
 template <>
 struct Coop<Fp> {
-#if GM_COOP_F64
-  using A = FpOutF64;
-#else
   using A = FpOut;
-#endif
   static constexpr int LANES = 4;
   GM_DEVI static void add(xyzz_t<A> &acc, const xyzz_t<A> &o) { q_add<A>(acc, o); }
   GM_DEVI static void dbl(xyzz_t<A> &p) { q_dbl<A>(p); }

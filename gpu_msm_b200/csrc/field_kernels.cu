@@ -77,8 +77,7 @@ int launch_field(gm_stream_t stream, uint32_t gpu_index, void *c, const void *a,
 
 // IMAD-pipe throughput probe: 16 independent accumulator chains per thread.
 // mode 0 issues 8 mad.lo.u32 + 8 mad.hi.u32 per iteration (the lo/hi mix of a
-// Montgomery product), mode 1 issues 16 mad.lo.u32, mode 2 issues 16
-// fma.rn.f64 (the FP64 pipe of the FP64 Montgomery product).  Each chain depends only
+// Montgomery product), mode 1 issues 16 mad.lo.u32.  Each chain depends only
 // on its own previous value.  Used to measure the integer multiply-add
 // ceiling that the MSM roofline is quoted against.
 __global__ void __launch_bounds__(256) k_imad_probe(uint32_t *__restrict__ sink, int iters, uint32_t seed, int mode) {
@@ -94,23 +93,11 @@ __global__ void __launch_bounds__(256) k_imad_probe(uint32_t *__restrict__ sink,
         asm volatile("mad.hi.u32 %0, %0, %1, %2;" : "+r"(a[k + 1]) : "r"(m), "r"(c));
       }
     }
-  } else if (mode == 1) {
+  } else {
     for (int it = 0; it < iters; it++) {
 #pragma unroll
       for (int k = 0; k < 16; k++) asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(a[k]) : "r"(m), "r"(c));
     }
-  } else {
-    // mode 2: 16 independent fma.rn.f64 chains (the FP64-pipe ceiling)
-    double d[16];
-#pragma unroll
-    for (int k = 0; k < 16; k++) d[k] = (double)a[k];
-    const double dm = 1.0 + 1.0 / (double)m, dc = (double)c;
-    for (int it = 0; it < iters; it++) {
-#pragma unroll
-      for (int k = 0; k < 16; k++) asm volatile("fma.rn.f64 %0, %0, %1, %2;" : "+d"(d[k]) : "d"(dm), "d"(dc));
-    }
-#pragma unroll
-    for (int k = 0; k < 16; k++) a[k] = (uint32_t)__double_as_longlong(d[k]);
   }
   uint32_t x = 0;
 #pragma unroll
@@ -147,14 +134,6 @@ int gm_profile_collect(char *names, int names_len, float *ms, int max) {
 }
 
 int64_t gm_launch_count_reset(void) { return gm::launches_and_reset(); }
-
-int gm_set_fp64_products(int on) {
-  gm::set_fp64_products(on != 0);
-  return gm::GM_OK;
-}
-
-int gm_fp64_products(void) { return gm::fp64_products() ? 1 : 0; }
-
 
 int gm_fp_mont_mul_array(gm_stream_t stream, uint32_t gpu_index, Fp *d_c, const Fp *d_a, const Fp *d_b, int64_t n) {
   return launch_field<gm::Fp, MONT_MUL>(stream, gpu_index, d_c, d_a, d_b, n);

@@ -65,7 +65,7 @@ void free_plan(gm_batch_plan *p) {
 
 // Validates the batch, groups MSMs by window width and computes each class's
 // layout; d64[k] / idx[k] receive class k's descriptors
-// (point_start | base_off | sc_off, and out_index).
+// (point_start | base_off | sc_off, and out_index | tile_first).
 int build_classes(const gm_bases *b, int scalar_limbs, int count, const int64_t *sizes, const int64_t *base_offsets,
                   const int32_t *window_bits, gm::BatchPlan &plan, std::vector<std::vector<int64_t>> &d64,
                   std::vector<std::vector<int32_t>> &idx) {
@@ -114,7 +114,10 @@ int build_classes(const gm_bases *b, int scalar_limbs, int count, const int64_t 
     gm::BatchClassPlan cp;
     cp.c = kv.first;
     cp.count = (int)kv.second.size();
-    for (int i : kv.second) cp.P += sizes[i];
+    for (int i : kv.second) {
+      cp.P += sizes[i];
+      cp.tilesA += (sizes[i] + gm::SA_TP - 1) / gm::SA_TP;
+    }
     if (const auto *t = b->table_for(cp.c, gm::windows_for(cp.c, scalar_limbs))) {
       cp.pc_table = t->table;
       cp.pc_stride = b->n;
@@ -137,10 +140,16 @@ int build_classes(const gm_bases *b, int scalar_limbs, int count, const int64_t 
       gm::set_last_error("batch class too large for 32-bit entry offsets");
       return gm::GM_ERR_ARG;
     }
+    if (cp.tilesA >= (int64_t)INT32_MAX) {
+      gm::set_last_error("batch class has too many sort tiles");
+      return gm::GM_ERR_ARG;
+    }
     std::vector<int64_t> &v = d64[k];
     v.assign(3 * (size_t)cp.count + 1, 0);
-    idx[k].assign(cp.count, 0);
+    // out_index[count] | tile_first[count + 1]
+    idx[k].assign(2 * (size_t)cp.count + 1, 0);
     int64_t acc = 0;
+    int32_t tiles = 0;
     for (int j = 0; j < cp.count; j++) {
       const int i = kv.second[j];
       v[j] = acc;
@@ -148,8 +157,11 @@ int build_classes(const gm_bases *b, int scalar_limbs, int count, const int64_t 
       v[cp.count + 1 + j] = base_offsets ? base_offsets[i] : 0;
       v[2 * cp.count + 1 + j] = sc_row[i];
       idx[k][j] = i;
+      idx[k][cp.count + j] = tiles;
+      tiles += (int32_t)((sizes[i] + gm::SA_TP - 1) / gm::SA_TP);
     }
     v[cp.count] = acc;
+    idx[k][2 * (size_t)cp.count] = tiles;
     k++;
   }
   return gm::GM_OK;

@@ -21,18 +21,21 @@ struct BatchClassPlan {
   DigitParams dp{};
   int count = 0;        // MSMs in this class
   int64_t P = 0;        // points in this class
-  int64_t K = 0, nb = 0, nthreads = 0;
-  bool fp64 = false;    // accumulation product mode, fixed when the plan is made
+  int64_t K = 0, nthreads = 0;
+  int64_t tilesA = 0;   // pass-A sort tiles (SA_TP points, one MSM each)
+  SortLayout sl;
   RedLayout rl;
   int64_t long_cap = 0;
   // fixed-base window table (precomputed mode): record w*pc_stride + base
   const uint4 *pc_table = nullptr;
   int64_t pc_stride = 0;
-  size_t o_counts = 0, o_offsets = 0, o_bsum = 0, o_entries = 0, o_buckets = 0, o_head = 0, o_tail = 0, o_hk = 0,
-         o_tk = 0, o_longq = 0, o_err = 0;
+  size_t o_offsets = 0, o_entries = 0, o_buckets = 0, o_head = 0, o_tail = 0, o_hk = 0, o_tk = 0, o_longq = 0,
+         o_err = 0;
   size_t ws_bytes = 0;
   char *ws = nullptr;       // workspace (owned)
-  char *desc = nullptr;     // point_start | base_off | sc_off | out_index (owned)
+  // descriptors (owned): int64 point_start[count+1] | base_off[count] |
+  // sc_off[count], then int32 out_index[count] | tile_first[count+1]
+  char *desc = nullptr;
   cudaStream_t stream = nullptr;
   cudaEvent_t done = nullptr;
 };
@@ -57,22 +60,19 @@ void batch_class_layout(BatchClassPlan &cp, int limbs, int sms, int dev) {
   // precomputed mode: one bucket set per MSM (no window index in the key)
   const int64_t groups = (int64_t)cp.count * (cp.pc_stride ? 1 : cp.dp.W);
   cp.K = groups * cp.dp.B;
-  cp.nb = (cp.K + SCAN_TILE - 1) / SCAN_TILE;
-  cp.fp64 = acc_fp64<F>();
-  cp.nthreads = (int64_t)sms * acc_blocks_per_sm<F>(dev, cp.fp64) * ACC_THREADS;
+  cp.nthreads = (int64_t)sms * acc_blocks_per_sm<F>(dev) * ACC_THREADS;
   const int64_t max_entries = cp.P * cp.dp.W;
   if (cp.nthreads > max_entries) cp.nthreads = std::max<int64_t>(1, (max_entries + 127) / 128 * 128);
   Carve cv;
-  cp.o_counts = cv.take<uint32_t>(cp.K);
   cp.o_offsets = cv.take<uint32_t>(cp.K + 1);
-  cp.o_bsum = cv.take<uint32_t>(cp.nb);
   cp.o_entries = cv.take<uint32_t>((size_t)std::max<int64_t>(1, max_entries));
+  cp.sl.plan(cp.dp, cp.count, cp.P, cp.tilesA, cp.pc_stride != 0, cv);
   cp.o_buckets = cv.take<xyzz_t<F>>(cp.K);
   cp.o_head = cv.take<xyzz_t<F>>(cp.nthreads);
   cp.o_tail = cv.take<xyzz_t<F>>(cp.nthreads);
   cp.o_hk = cv.take<int32_t>(cp.nthreads);
   cp.o_tk = cv.take<int32_t>(cp.nthreads);
-  cp.rl.plan<F>(groups, cp.dp.B, (int64_t)sms * level0_blocks_per_sm<F>(dev) * 128, cv);
+  cp.rl.plan<F>(groups, cp.dp.B, (int64_t)sms * level0_blocks_per_sm<F>(dev) * 128, cv, coop_wave_threads<F>(dev, sms));
   cp.rl.sms = sms;
   cp.rl.dev = dev;
   cp.long_cap = cp.nthreads / FIX_SHORT + 1;
@@ -87,9 +87,7 @@ int batch_class_run(const BatchPlan &plan, const BatchClassPlan &cp, cudaStream_
                     uint64_t *results) {
   if (cp.count == 0) return GM_OK;
   char *ws = cp.ws;
-  auto *counts = (uint32_t *)(ws + cp.o_counts);
   auto *offsets = (uint32_t *)(ws + cp.o_offsets);
-  auto *bsum = (uint32_t *)(ws + cp.o_bsum);
   auto *entries = (uint32_t *)(ws + cp.o_entries);
   auto *buckets = (xyzz_t<F> *)(ws + cp.o_buckets);
   auto *head = (xyzz_t<F> *)(ws + cp.o_head);
@@ -98,28 +96,23 @@ int batch_class_run(const BatchPlan &plan, const BatchClassPlan &cp, cudaStream_
   auto *tk = (int32_t *)(ws + cp.o_tk);
   auto *err = (uint32_t *)(ws + cp.o_err);
   auto *long_q = (int32_t *)(ws + cp.o_longq);
-  MultiDesc md;
-  md.point_start = (const int64_t *)cp.desc;
-  md.base_off = md.point_start + cp.count + 1;
-  md.sc_off = md.base_off + cp.count;
-  md.count = cp.count;
-  const int32_t *out_index = (const int32_t *)(md.sc_off + cp.count);
+  SortDesc sd;
+  sd.point_start = (const int64_t *)cp.desc;
+  sd.base_off = sd.point_start + cp.count + 1;
+  sd.sc_off = sd.base_off + cp.count;
+  sd.count = cp.count;
+  sd.pc_stride = cp.pc_stride;
+  const int32_t *out_index = (const int32_t *)(sd.sc_off + cp.count);
+  sd.tile_first = out_index + cp.count;
 
   int launches = 0;
-  GM_CHECK(cudaMemsetAsync(counts, 0, cp.K * sizeof(uint32_t), s));
   GM_CHECK(cudaMemsetAsync(err, 0, sizeof(uint32_t), s));
   GM_CHECK(cudaMemsetAsync(long_q, 0, sizeof(int32_t), s));
-  k_count_multi<<<grid_for(cp.P, 256), 256, 0, s>>>(scalars, cp.P, md, cp.dp, cp.pc_stride, counts);
-  GM_CHECK_LAUNCH("k_count_multi");
-  k_scan_blocksum<<<(unsigned)cp.nb, SCAN_THREADS, 0, s>>>(counts, cp.K, bsum);
-  k_scan_top<<<1, SCAN_THREADS, 0, s>>>(bsum, (int)cp.nb);
-  k_scan_final<<<(unsigned)cp.nb, SCAN_THREADS, 0, s>>>(counts, cp.K, bsum, offsets);
-  GM_CHECK_LAUNCH("k_scan");
-  k_scatter_multi<<<grid_for(cp.P, 256), 256, 0, s>>>(scalars, cp.P, md, cp.dp, cp.pc_stride, offsets, counts,
-                                                      entries);
-  GM_CHECK_LAUNCH("k_scatter_multi");
-  launches += 5;
-  acc_launch<F>(cp.fp64, grid_for(cp.nthreads, ACC_THREADS), s, cp.pc_table ? cp.pc_table : plan.bases, entries,
+  {
+    const cudaError_t e = sort_launch(s, cp.sl, ws, scalars, sd, cp.K, offsets, entries, &launches);
+    if (e != cudaSuccess) return record_error(e, "batch sort");
+  }
+  acc_launch<F>(grid_for(cp.nthreads, ACC_THREADS), s, cp.pc_table ? cp.pc_table : plan.bases, entries,
                 offsets, cp.K, cp.nthreads, buckets, head, tail, hk, tk);
   GM_CHECK_LAUNCH("k_accumulate");
   launches++;

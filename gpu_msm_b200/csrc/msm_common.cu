@@ -9,7 +9,6 @@
 // pool so concurrent calls on different streams never share scratch.
 #include <cuda_runtime.h>
 
-#include <atomic>
 #include <cstdlib>
 
 #include <algorithm>
@@ -40,25 +39,6 @@ int record_error(cudaError_t e, const char *where) {
 const char *last_error() { return g_last_error.c_str(); }
 
 void set_last_error(const char *msg) { g_last_error = msg; }
-
-#ifndef GM_ACC_F64
-#define GM_ACC_F64 0
-#endif
-namespace {
-std::atomic<int> g_fp64_products{-1};  // -1: not read yet
-}
-bool fp64_products() {
-  int v = g_fp64_products.load(std::memory_order_relaxed);
-  if (v < 0) {
-    const char *env = getenv("GM_FP64_PRODUCTS");
-    v = env ? (atoi(env) != 0) : (GM_ACC_F64 != 0);
-    int expect = -1;
-    g_fp64_products.compare_exchange_strong(expect, v);
-    v = g_fp64_products.load(std::memory_order_relaxed);
-  }
-  return v != 0;
-}
-void set_fp64_products(bool on) { g_fp64_products.store(on ? 1 : 0, std::memory_order_relaxed); }
 
 #define GM_CHECK(call)                                                  \
   do {                                                                  \

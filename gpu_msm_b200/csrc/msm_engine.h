@@ -43,12 +43,6 @@ int pinned_acquire(void **p);
 void pinned_release(void *p);
 int enqueue_pinned_release(cudaStream_t s, void *slot);
 void set_host_tail_enabled(bool on);
-// Product mode of the G1 bucket accumulation: false (default) = integer CIOS
-// product on the IMAD pipe, true = the bit-identical product on the FP64
-// pipe.  The initial value comes from the environment variable
-// GM_FP64_PRODUCTS (1 = on), else from the build (GM_ACC_F64).
-bool fp64_products();
-void set_fp64_products(bool on);
 // kernel launches issued by this host thread since the last reset
 void count_launches(int k);
 int64_t launches_and_reset();

@@ -12,6 +12,7 @@
 #include "msm_engine.h"
 #include "msm_kernels.cuh"
 #include "msm_reduce.cuh"
+#include "msm_sort.cuh"
 
 namespace gm {
 
@@ -47,25 +48,18 @@ template <class F>
 struct MsmLayout {
   DigitParams dp;
   int64_t K = 0, nthreads = 0, n = 0;
-  int L1 = 8;     // buckets per reduction segment
-  int FAN = 4;    // fan-in of the segment-share tree
-  int nseg = 0;   // reduction segments per window
-  size_t o_counts, o_offsets, o_bsum, o_entries, o_buckets, o_head, o_tail, o_hk, o_tk, o_red[3], o_err, o_packed;
-  size_t o_longq = 0;
+  size_t o_offsets, o_entries, o_buckets, o_head, o_tail, o_hk, o_tk, o_err, o_packed, o_longq;
   size_t bytes = 0;
-  int64_t nb = 0;
-  int64_t red_elems = 0;
   int64_t long_cap = 0;
   bool need_pack = false;
-  // leveled reduction (k_red_level0/1 + quad tree) and split fix-up; the
-  // allocation-free entry point keeps the segment reduction
-  bool leveled = false;
+  SortLayout sl;
   RedLayout rl;
 
-  // level0_wave: threads of k_red_level0 resident at once (leveled only)
-  void plan(int64_t n_, int limbs, int c, int sms, int acc_blocks_per_sm, bool pack, bool leveled_ = false,
-            int64_t level0_wave = 0) {
-    leveled = leveled_;
+  // slice_threads: accumulation slices (one per thread of a single wave);
+  // level0_wave / coop_wave: threads of k_red_level0 / k_red_level1 resident
+  // at once
+  void plan(int64_t n_, int limbs, int c, int64_t slice_threads, bool pack, int64_t level0_wave,
+            int64_t coop_wave) {
     n = n_;
     need_pack = pack;
     dp.c = c;
@@ -73,35 +67,22 @@ struct MsmLayout {
     dp.B = 1 << (c - 1);
     dp.limbs = limbs;
     K = (int64_t)dp.W * dp.B;
-    nb = (K + SCAN_TILE - 1) / SCAN_TILE;
-    nthreads = (int64_t)sms * std::max(1, acc_blocks_per_sm) * ACC_THREADS;
+    nthreads = std::max<int64_t>(ACC_THREADS, slice_threads);
     // never more slices than entries
     const int64_t max_entries = n * dp.W;
     if (nthreads > max_entries) nthreads = std::max<int64_t>(1, (max_entries + 127) / 128 * 128);
-    L1 = std::min(L1, dp.B);
-    nseg = (dp.B + L1 - 1) / L1;
-    red_elems = (int64_t)dp.W * nseg;
     Carve cv;
-    o_counts = cv.take<uint32_t>(K);
     o_offsets = cv.take<uint32_t>(K + 1);
-    o_bsum = cv.take<uint32_t>(nb);
     o_entries = cv.take<uint32_t>((size_t)std::max<int64_t>(1, max_entries));
+    sl.plan(dp, 1, n, (n + SA_TP - 1) / SA_TP, /*tabled=*/false, cv);
     o_buckets = cv.take<xyzz_t<F>>(K);
     o_head = cv.take<xyzz_t<F>>(nthreads);
     o_tail = cv.take<xyzz_t<F>>(nthreads);
     o_hk = cv.take<int32_t>(nthreads);
     o_tk = cv.take<int32_t>(nthreads);
-    if (leveled) {
-      rl.plan<F>(dp.W, dp.B, level0_wave, cv);
-      rl.sms = sms;
-      long_cap = nthreads / FIX_SHORT + 1;
-      o_longq = cv.take<int32_t>((size_t)(1 + long_cap));
-      o_red[0] = o_red[1] = o_red[2] = 0;
-    } else {
-      o_red[0] = cv.take<xyzz_t<F>>(red_elems);
-      o_red[1] = cv.take<xyzz_t<F>>((red_elems + FAN - 1) / FAN + dp.W);
-      o_red[2] = cv.take<xyzz_t<F>>((red_elems + FAN - 1) / FAN + dp.W);
-    }
+    rl.plan<F>(dp.W, dp.B, level0_wave, cv, coop_wave);
+    long_cap = nthreads / FIX_SHORT + 1;
+    o_longq = cv.take<int32_t>((size_t)(1 + long_cap));
     o_err = cv.take<uint32_t>(4);
     o_packed = pack ? cv.take<uint4>((size_t)n * Rec<F>::U4) : 0;
     bytes = cv.off;
@@ -122,7 +103,7 @@ struct AccOccupancy {
   size_t smem = 0;    // dynamic shared memory of a launch
 };
 
-template <class F, bool FP64>
+template <class F>
 static AccOccupancy acc_occupancy(int dev) {
   static std::mutex mu;
   static AccOccupancy cached[64];
@@ -133,17 +114,15 @@ static AccOccupancy acc_occupancy(int dev) {
     size_t smem = acc_smem_bytes<F>();
     int per_sm_smem = 0, b = 0;
     cudaDeviceGetAttribute(&per_sm_smem, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
-    cudaFuncSetAttribute(k_accumulate<F, FP64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_accumulate<F, FP64>, ACC_THREADS, smem) != cudaSuccess)
-      b = 1;
+    cudaFuncSetAttribute(k_accumulate<F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_accumulate<F>, ACC_THREADS, smem) != cudaSuccess) b = 1;
     if (b > ACC_BLOCKS_MAX && per_sm_smem > 0) {
       // (ACC_BLOCKS_MAX + 1) blocks must not fit in the SM's shared memory
       const size_t pad = (size_t)per_sm_smem / (ACC_BLOCKS_MAX + 1) + 1024;
-      if (cudaFuncSetAttribute(k_accumulate<F, FP64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pad) ==
+      if (cudaFuncSetAttribute(k_accumulate<F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pad) ==
           cudaSuccess)
         smem = pad;
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_accumulate<F, FP64>, ACC_THREADS, smem) !=
-          cudaSuccess)
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_accumulate<F>, ACC_THREADS, smem) != cudaSuccess)
         b = 1;
     }
     o.smem = smem;
@@ -152,42 +131,19 @@ static AccOccupancy acc_occupancy(int dev) {
   return o;
 }
 
-template <class F, bool FP64>
-static int acc_blocks_per_sm_mode(int dev) {
-  return acc_occupancy<F, FP64>(dev).blocks;
-}
-
-// Whether the accumulation of group F uses FP64-pipe products (G1 only, when
-// the run-time mode is on).
 template <class F>
-static bool acc_fp64() {
-  return F::LIMBS == NL && fp64_products();
+static int acc_blocks_per_sm(int dev) {
+  return acc_occupancy<F>(dev).blocks;
 }
 
 template <class F>
-static int acc_blocks_per_sm(int dev, bool fp64) {
-  if constexpr (F::LIMBS == NL) {
-    if (fp64) return acc_blocks_per_sm_mode<F, true>(dev);
-  }
-  return acc_blocks_per_sm_mode<F, false>(dev);
-}
-
-// k_accumulate in the chosen product mode
-template <class F>
-static void acc_launch(bool fp64, unsigned grid, cudaStream_t s, const uint4 *bases, const uint32_t *entries,
+static void acc_launch(unsigned grid, cudaStream_t s, const uint4 *bases, const uint32_t *entries,
                        const uint32_t *offsets, int64_t K, int64_t nthreads, xyzz_t<F> *buckets, xyzz_t<F> *head,
                        xyzz_t<F> *tail, int32_t *hk, int32_t *tk) {
   int dev = 0;
   cudaGetDevice(&dev);
-  if constexpr (F::LIMBS == NL) {
-    if (fp64) {
-      k_accumulate<F, true><<<grid, ACC_THREADS, acc_occupancy<F, true>(dev).smem, s>>>(
-          bases, entries, offsets, K, nthreads, buckets, head, tail, hk, tk);
-      return;
-    }
-  }
-  k_accumulate<F, false><<<grid, ACC_THREADS, acc_occupancy<F, false>(dev).smem, s>>>(
-      bases, entries, offsets, K, nthreads, buckets, head, tail, hk, tk);
+  k_accumulate<F><<<grid, ACC_THREADS, acc_occupancy<F>(dev).smem, s>>>(bases, entries, offsets, K, nthreads,
+                                                                          buckets, head, tail, hk, tk);
 }
 
 static inline unsigned grid_for(int64_t n, int block) { return (unsigned)((n + block - 1) / block); }
@@ -205,6 +161,22 @@ static int level0_blocks_per_sm(int dev) {
     cached[dev] = std::max(1, b);
   }
   return cached[dev];
+}
+
+// Threads of the cooperative level-1 reduction kernel resident at once on
+// the device (cached per device).
+template <class F>
+static int64_t coop_wave_threads(int dev, int sms) {
+  static std::mutex mu;
+  static int cached[64] = {0};
+  std::lock_guard<std::mutex> lk(mu);
+  if (dev < 0 || dev >= 64) dev = 0;
+  if (cached[dev] == 0) {
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_red_level1<F>, 128, 0) != cudaSuccess) b = 1;
+    cached[dev] = std::max(1, b);
+  }
+  return (int64_t)sms * cached[dev] * 128;
 }
 
 // Split fix-up: short runs serially, long runs by a block-level tree.
@@ -258,47 +230,50 @@ int reduce_launch(cudaStream_t s, const RedLayout &rl, const xyzz_t<F> *buckets,
   return GM_OK;
 }
 
-// Runs the whole pipeline.  bases: packed records (or null to pack from
-// ref_points), scalars: device u64 limbs, out: reference projective layout.
-// bases_ready (optional): an event the stream waits for after the sort and
-// before it first reads the bases.
+// Plans the workspace of one MSM on device dev.  slice_threads 0: one
+// accumulation slice per thread of a full wave (ACC_BLOCKS_MAX blocks per SM).
 template <class F>
-int msm_launch(cudaStream_t s, int dev, const uint4 *bases, const uint64_t *ref_points, int to_mont,
-               const uint64_t *scalars, int limbs, int64_t n, uint64_t *out_proj, int c_override,
-               uint32_t *err_out, cudaEvent_t bases_ready) {
-  constexpr int H = F::LIMBS / 2;  // u64 words per coordinate
-  if (n == 0) {
-    GM_CHECK(cudaMemsetAsync(out_proj, 0, 3 * H * sizeof(uint64_t), s));
-    return GM_OK;
-  }
-  if (limbs < 1 || limbs > MAX_SCALAR_LIMBS || n < 0 || n > (int64_t)INT32_MAX) {
+int msm_plan(MsmLayout<F> &lay, int dev, int64_t n, int limbs, int c, bool pack, int64_t slice_threads) {
+  if (limbs < 1 || limbs > MAX_SCALAR_LIMBS || n < 1 || n > (int64_t)INT32_MAX) {
     set_last_error("invalid scalar_limbs or n");
+    return GM_ERR_ARG;
+  }
+  if (c < 2 || c > 20) {
+    set_last_error("window width out of range");
     return GM_ERR_ARG;
   }
   int sms = 0;
   int rc = device_sm_count(dev, &sms);
   if (rc) return rc;
-  const int c = c_override > 0 ? c_override : default_window(sizeof(typename F::T) == sizeof(fp_t) ? 1 : 2, n, limbs);
-  if (c < 2 || c > 20) {
-    set_last_error("window width out of range");
-    return GM_ERR_ARG;
-  }
-  MsmLayout<F> lay;
-  const bool fp64 = acc_fp64<F>();
-  lay.plan(n, limbs, c, sms, acc_blocks_per_sm<F>(dev, fp64), bases == nullptr, /*leveled=*/true,
-           (int64_t)sms * level0_blocks_per_sm<F>(dev) * 128);
+  if (slice_threads <= 0) slice_threads = (int64_t)sms * acc_blocks_per_sm<F>(dev) * ACC_THREADS;
+  lay.plan(n, limbs, c, slice_threads, pack, (int64_t)sms * level0_blocks_per_sm<F>(dev) * 128,
+           coop_wave_threads<F>(dev, sms));
+  lay.rl.sms = sms;
   lay.rl.dev = dev;
   if ((uint64_t)n * lay.dp.W >= (1ull << 32)) {
     set_last_error("too many (point, window) entries for 32-bit offsets");
     return GM_ERR_ARG;
   }
-  char *ws = nullptr;
-  rc = pool_alloc(dev, s, lay.bytes, (void **)&ws);
-  if (rc) return rc;
+  return GM_OK;
+}
 
-  auto *counts = (uint32_t *)(ws + lay.o_counts);
+// Enqueues the whole pipeline of one planned MSM on s, in the workspace ws
+// (lay.bytes, 256-byte aligned); allocates nothing itself.  bases: packed
+// records, or null to pack from ref_points (reference layout; to_mont converts
+// standard-form points).  out_proj receives the projective result in the
+// reference layout.  host_tail: the window combination runs on the host (a
+// pinned staging slot and a stream-ordered host function); otherwise, and
+// always while s is being captured, on the device.  err_out (optional,
+// device) receives the consistency flag of the fix-up (0 = ok).  bases_ready
+// (optional): an event the stream waits for after the sort, before the bases
+// are first read.
+template <class F>
+int msm_run(cudaStream_t s, const MsmLayout<F> &lay, char *ws, const uint4 *bases, const uint64_t *ref_points,
+            int to_mont, const uint64_t *scalars, uint64_t *out_proj, bool host_tail, uint32_t *err_out,
+            cudaEvent_t bases_ready) {
+  constexpr int H = F::LIMBS / 2;  // u64 words per coordinate
+  const int64_t n = lay.n;
   auto *offsets = (uint32_t *)(ws + lay.o_offsets);
-  auto *bsum = (uint32_t *)(ws + lay.o_bsum);
   auto *entries = (uint32_t *)(ws + lay.o_entries);
   auto *buckets = (xyzz_t<F> *)(ws + lay.o_buckets);
   auto *head = (xyzz_t<F> *)(ws + lay.o_head);
@@ -306,23 +281,19 @@ int msm_launch(cudaStream_t s, int dev, const uint4 *bases, const uint64_t *ref_
   auto *hk = (int32_t *)(ws + lay.o_hk);
   auto *tk = (int32_t *)(ws + lay.o_tk);
   auto *err = (uint32_t *)(ws + lay.o_err);
+  auto *long_q = (int32_t *)(ws + lay.o_longq);
   profile_mark(s, "start");
   int launches = 0;
   // the sort needs only the scalars; the bases are packed after it, so a
   // caller that is still copying them in can overlap that copy with the sort
-  GM_CHECK(cudaMemsetAsync(counts, 0, lay.K * sizeof(uint32_t), s));
   GM_CHECK(cudaMemsetAsync(err, 0, sizeof(uint32_t), s));
-  auto *long_q = (int32_t *)(ws + lay.o_longq);
   GM_CHECK(cudaMemsetAsync(long_q, 0, sizeof(int32_t), s));
-  k_count<<<grid_for(n, 256), 256, 0, s>>>(scalars, n, lay.dp, counts);
-  GM_CHECK_LAUNCH("k_count");
-  k_scan_blocksum<<<(unsigned)lay.nb, SCAN_THREADS, 0, s>>>(counts, lay.K, bsum);
-  k_scan_top<<<1, SCAN_THREADS, 0, s>>>(bsum, (int)lay.nb);
-  k_scan_final<<<(unsigned)lay.nb, SCAN_THREADS, 0, s>>>(counts, lay.K, bsum, offsets);
-  GM_CHECK_LAUNCH("k_scan");
-  k_scatter<<<grid_for(n, 256), 256, 0, s>>>(scalars, n, lay.dp, offsets, counts, entries);
-  GM_CHECK_LAUNCH("k_scatter");
-  launches += 5;
+  {
+    SortDesc sd;
+    sd.n_single = n;
+    const cudaError_t e = sort_launch(s, lay.sl, ws, scalars, sd, lay.K, offsets, entries, &launches);
+    if (e != cudaSuccess) return record_error(e, "sort");
+  }
   profile_mark(s, "sort");
   if (bases_ready) GM_CHECK(cudaStreamWaitEvent(s, bases_ready, 0));
   if (bases == nullptr) {
@@ -333,13 +304,13 @@ int msm_launch(cudaStream_t s, int dev, const uint4 *bases, const uint64_t *ref_
     launches++;
     profile_mark(s, "pack");
   }
-  acc_launch<F>(fp64, grid_for(lay.nthreads, ACC_THREADS), s, bases, entries, offsets, lay.K, lay.nthreads, buckets,
-                head, tail, hk, tk);
+  acc_launch<F>(grid_for(lay.nthreads, ACC_THREADS), s, bases, entries, offsets, lay.K, lay.nthreads, buckets, head,
+                tail, hk, tk);
   GM_CHECK_LAUNCH("k_accumulate");
   launches++;
   profile_mark(s, "accumulate");
-  rc = fixup_launch<F>(s, offsets, lay.K, lay.nthreads, buckets, head, tail, hk, tk, err, long_q, lay.long_cap,
-                       &launches);
+  int rc = fixup_launch<F>(s, offsets, lay.K, lay.nthreads, buckets, head, tail, hk, tk, err, long_q, lay.long_cap,
+                           &launches);
   if (rc) return rc;
   profile_mark(s, "fixup");
 
@@ -353,19 +324,45 @@ int msm_launch(cudaStream_t s, int dev, const uint4 *bases, const uint64_t *ref_
   // latency per product) unless the stream is being captured into a graph
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   GM_CHECK(cudaStreamIsCapturing(s, &cap));
-  if (cap == cudaStreamCaptureStatusNone && host_tail_enabled()) {
-    rc = enqueue_host_tail(s, F::LIMBS == NL ? 1 : 2, src, W, c, out_proj);
+  if (host_tail && cap == cudaStreamCaptureStatusNone) {
+    rc = enqueue_host_tail(s, F::LIMBS == NL ? 1 : 2, src, W, lay.dp.c, out_proj);
     if (rc) return rc;
   } else {
-    k_combine_quad<F><<<1, 32, 0, s>>>(src, 1, W, c, nullptr, out_proj);
+    k_combine_quad<F><<<1, 32, 0, s>>>(src, 1, W, lay.dp.c, nullptr, out_proj);
     GM_CHECK_LAUNCH("k_combine_quad");
     launches++;
   }
   profile_mark(s, "combine");
   count_launches(launches);
   if (err_out) GM_CHECK(cudaMemcpyAsync(err_out, err, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
-  GM_CHECK(cudaFreeAsync(ws, s));
   return GM_OK;
+}
+
+// The whole pipeline with its workspace from the device's stream-ordered
+// pool, released on s after the last kernel (also when an enqueue fails).
+// c_override 0: the window width from the cost model.
+template <class F>
+int msm_launch(cudaStream_t s, int dev, const uint4 *bases, const uint64_t *ref_points, int to_mont,
+               const uint64_t *scalars, int limbs, int64_t n, uint64_t *out_proj, int c_override,
+               uint32_t *err_out, cudaEvent_t bases_ready) {
+  constexpr int H = F::LIMBS / 2;
+  if (n == 0) {
+    if (err_out) GM_CHECK(cudaMemsetAsync(err_out, 0, sizeof(uint32_t), s));
+    GM_CHECK(cudaMemsetAsync(out_proj, 0, 3 * H * sizeof(uint64_t), s));
+    return GM_OK;
+  }
+  const int c = c_override > 0 ? c_override : default_window(sizeof(typename F::T) == sizeof(fp_t) ? 1 : 2, n, limbs);
+  MsmLayout<F> lay;
+  int rc = msm_plan<F>(lay, dev, n, limbs, c, bases == nullptr, 0);
+  if (rc) return rc;
+  char *ws = nullptr;
+  rc = pool_alloc(dev, s, lay.bytes, (void **)&ws);
+  if (rc) return rc;
+  rc = msm_run<F>(s, lay, ws, bases, ref_points, to_mont, scalars, out_proj, host_tail_enabled(), err_out,
+                  bases_ready);
+  const cudaError_t e = cudaFreeAsync(ws, s);
+  if (rc) return rc;
+  return e == cudaSuccess ? GM_OK : record_error(e, "cudaFreeAsync(workspace)");
 }
 
 }  // namespace gm

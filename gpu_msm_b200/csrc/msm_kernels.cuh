@@ -4,22 +4,21 @@
 // pdroalves/gpu_msm src/curve.cu:2538-2677 and the affine multi-limb path
 // src/curve.cu:2763-2820):
 //
-//  1. k_count      signed c-bit digit decomposition of every scalar; count the
-//                  non-zero digits per global bucket key  key = w*B + |d|-1
-//                  (B = 2^(c-1) buckets per window).
-//  2. k_scan_*     exclusive prefix sum of the counts -> bucket offsets.
-//  3. k_scatter    counting-sort scatter: the (point, sign) entries land
-//                  grouped by bucket key (one radix pass over all windows).
+//  1-3. k_sort_*  signed c-bit digit decomposition of every scalar and a
+//                  stable radix sort of the (point, sign) entries by bucket
+//                  key  key = w*B + |d|-1  (B = 2^(c-1) buckets per window),
+//                  with the bucket offsets (msm_sort.cuh; k_scan_* below are
+//                  its prefix sums).
 //  4. k_accumulate every thread sums an equal-length slice of the sorted
 //                  entries with XYZZ mixed additions; buckets that fit in a
 //                  slice are written directly, the edge pieces of buckets that
 //                  straddle slices are written as partials.
-//  5. k_fixup      the slice that opened a straddling bucket adds the
-//                  partials of the following slices.
-//  6. k_reduce     per window, sum_b b*Bucket_b by segmented running sums,
-//                  applied level by level until one (R, A) pair per window
-//                  remains; the window sum is R + A.
-//  7. k_combine    result = sum_w 2^(c*w) * S_w by Horner, converted to the
+//  5. k_fixup_*    the slice that opened a straddling bucket adds the
+//                  partials of the following slices (msm_reduce.cuh).
+//  6. k_red_*      per window, sum_b (b+1)*Bucket_b by segmented running sums
+//                  and a quad fan-in tree (msm_reduce.cuh).
+//  7. combine      result = sum_w 2^(c*w) * S_w by Horner (host tail, or
+//                  k_combine_quad on the device), converted to the
 //                  reference's homogeneous projective output.
 //
 // Packed base records (written once by k_pack_*): affine x, y in Montgomery
@@ -29,7 +28,6 @@
 #pragma once
 #include <cstdint>
 
-#include "field_f64.cuh"
 #include "xyzz.cuh"
 
 namespace gm {
@@ -48,22 +46,10 @@ struct Rec<Fp2> {
 // Arithmetic policy with the field product out of line (same data types).
 template <class F>
 struct OutOfLine;
-// Build switch: Fp products of the reduction kernels on the FP64 pipe
-// (field_f64.cuh).  Off by default -- the path stays on integer instructions;
-// on, the G1 2^20 reduction measured 1.91 ms against 2.03 ms.
-#ifndef GM_OOL_F64
-#define GM_OOL_F64 0
-#endif
 template <>
 struct OutOfLine<Fp> {
-#if GM_OOL_F64
-  using type = FpOutF64;
-#else
   using type = FpOut;
-#endif
 };
-// G2 keeps the integer product: with its three Fp products on the FP64 pipe
-// the G2 2^18 reduction measured 3.01 ms against 2.98 ms.
 template <>
 struct OutOfLine<Fp2> {
   using type = Fp2Call;
@@ -72,17 +58,8 @@ struct OutOfLine<Fp2> {
 // Policy of the accumulation loop (one out-of-line product only).
 template <class F>
 struct AccPolicy;
-// G1 accumulation product: the integer CIOS product by default.  The
-// FP64-pipe product (field_f64.cuh, bit-identical) is chosen at run time
-// instead when set_fp64_products(true) -- see AccSel below; GM_ACC_F64 sets
-// that mode's initial value.  Measured on B200 for the G1 2^20 accumulation:
-// 11.10 ms with FP64-pipe products against 13.28 ms.  (Inside the G2 Fp2
-// product it measured 12.21 ms against 12.02 ms, so G2 has no FP64 mode.)
-#ifndef GM_ACC_F64
-#define GM_ACC_F64 0
-#endif
-// One product function only: squares on the integer pipe beside FP64-pipe
-// products (two out-of-line functions in the loop) measured 15.12 ms.
+// G1: the integer CIOS product out of line, squares through it too (one
+// product function in the loop).
 template <>
 struct AccPolicy<Fp> {
   using type = FpOutMulOnly;
@@ -94,17 +71,6 @@ struct AccPolicy<Fp> {
 template <>
 struct AccPolicy<Fp2> {
   using type = Fp2Call;
-};
-
-// Accumulation policy for the run-time product mode: FP64-pipe products for
-// G1 when FP64 is set, else AccPolicy's.
-template <class F, bool FP64>
-struct AccSel {
-  using type = typename AccPolicy<F>::type;
-};
-template <>
-struct AccSel<Fp, true> {
-  using type = FpOutF64;
 };
 
 template <class A, class B>
@@ -281,118 +247,6 @@ struct DigitParams {
   int limbs;   // u64 limbs per scalar
 };
 
-GM_DEVI uint32_t window_bits(const uint64_t s[MAX_SCALAR_LIMBS], int limbs, int off, int c) {
-  const int l = off >> 6, sh = off & 63;
-  if (l >= limbs) return 0;
-  uint64_t v = s[l] >> sh;
-  if (sh + c > 64 && l + 1 < limbs) v |= s[l + 1] << (64 - sh);
-  return (uint32_t)(v & ((1ull << c) - 1));
-}
-
-// Calls fn(w, d) for every non-zero signed digit d of the scalar, where
-// scalar = sum_w d_w 2^(c w) and |d_w| <= 2^(c-1).
-template <class Fn>
-GM_DEVI void for_each_digit(const uint64_t *__restrict__ scalar, const DigitParams &dp, Fn fn) {
-  uint64_t s[MAX_SCALAR_LIMBS];
-#pragma unroll
-  for (int l = 0; l < MAX_SCALAR_LIMBS; l++) s[l] = l < dp.limbs ? scalar[l] : 0;
-  uint32_t carry = 0;
-  for (int w = 0; w < dp.W; w++) {
-    const uint32_t v = window_bits(s, dp.limbs, w * dp.c, dp.c) + carry;
-    int d;
-    if (v > (uint32_t)dp.B) {
-      d = (int)v - 2 * dp.B;
-      carry = 1;
-    } else {
-      d = (int)v;
-      carry = 0;
-    }
-    if (d != 0) fn(w, d);
-  }
-}
-
-// The sort reads only the scalars: entries of bases at infinity are sorted
-// like any other and skipped by the accumulation.
-static __global__ void k_count(const uint64_t *__restrict__ scalars, int64_t n, DigitParams dp,
-                               uint32_t *__restrict__ counts) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  for_each_digit(scalars + i * dp.limbs, dp, [&](int w, int d) {
-    const int b = (d < 0 ? -d : d) - 1;
-    atomicAdd(&counts[w * dp.B + b], 1u);
-  });
-}
-
-// Consumes counts back down to zero; entry = (point index << 1) | negative.
-static __global__ void k_scatter(const uint64_t *__restrict__ scalars, int64_t n, DigitParams dp,
-                                 const uint32_t *__restrict__ offsets, uint32_t *__restrict__ counts,
-                                 uint32_t *__restrict__ entries) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  for_each_digit(scalars + i * dp.limbs, dp, [&](int w, int d) {
-    const int key = w * dp.B + (d < 0 ? -d : d) - 1;
-    const uint32_t rank = atomicSub(&counts[key], 1u) - 1u;
-    entries[offsets[key] + rank] = ((uint32_t)i << 1) | (d < 0 ? 1u : 0u);
-  });
-}
-
-// Many MSMs in one pipeline (batched mode).  MSM i owns the flattened point
-// ids [point_start[i], point_start[i+1]); its j-th point uses base record
-// base_off[i] + j of the shared table and scalar row sc_off[i] + j.  Its
-// bucket keys are i*W*B + w*B + |d|-1, so one counting sort, one
-// accumulation and one reduction serve every MSM of the batch.
-// With a fixed-base window table (pc_stride = table points n > 0) the window
-// index moves from the bucket key to the base record: keys are i*B + |d|-1
-// and the entry addresses record w*n + base of the table.
-struct MultiDesc {
-  const int64_t *point_start;  // [count + 1]
-  const int64_t *base_off;     // [count]
-  const int64_t *sc_off;       // [count]
-  int count;
-};
-
-GM_DEVI int msm_of(const int64_t *__restrict__ ps, int count, int64_t p) {
-  int lo = 0, hi = count;  // ps[lo] <= p < ps[hi]
-  while (hi - lo > 1) {
-    const int mid = (lo + hi) >> 1;
-    if (__ldg(ps + mid) <= p)
-      lo = mid;
-    else
-      hi = mid;
-  }
-  return lo;
-}
-
-static __global__ void k_count_multi(const uint64_t *__restrict__ scalars, int64_t P, MultiDesc md, DigitParams dp,
-                                     int64_t pc_stride, uint32_t *__restrict__ counts) {
-  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= P) return;
-  const int i = msm_of(md.point_start, md.count, p);
-  const int64_t j = p - __ldg(md.point_start + i);
-  const int64_t bi = __ldg(md.base_off + i) + j;
-  const int64_t kbase = (int64_t)i * (pc_stride ? 1 : dp.W) * dp.B;
-  for_each_digit(scalars + (__ldg(md.sc_off + i) + j) * dp.limbs, dp, [&](int w, int d) {
-    atomicAdd(&counts[kbase + (pc_stride ? 0 : (int64_t)w * dp.B) + (d < 0 ? -d : d) - 1], 1u);
-  });
-}
-
-static __global__ void k_scatter_multi(const uint64_t *__restrict__ scalars, int64_t P, MultiDesc md,
-                                       DigitParams dp, int64_t pc_stride, const uint32_t *__restrict__ offsets,
-                                       uint32_t *__restrict__ counts, uint32_t *__restrict__ entries) {
-  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= P) return;
-  const int i = msm_of(md.point_start, md.count, p);
-  const int64_t j = p - __ldg(md.point_start + i);
-  const int64_t bi = __ldg(md.base_off + i) + j;
-  const int64_t kbase = (int64_t)i * (pc_stride ? 1 : dp.W) * dp.B;
-  for_each_digit(scalars + (__ldg(md.sc_off + i) + j) * dp.limbs, dp, [&](int w, int d) {
-    const int64_t key = kbase + (pc_stride ? 0 : (int64_t)w * dp.B) + (d < 0 ? -d : d) - 1;
-    const uint32_t rank = atomicSub(&counts[key], 1u) - 1u;
-    const int64_t rec = pc_stride ? (int64_t)w * pc_stride + bi : bi;
-    entries[offsets[key] + rank] = ((uint32_t)rec << 1) | (d < 0 ? 1u : 0u);
-  });
-}
-
 // ---------------------------------------------------------------------------
 // 2. exclusive scan (three kernels, 1024 elements per block)
 // ---------------------------------------------------------------------------
@@ -558,14 +412,14 @@ struct StagedPoint {
 // laid out chunk-major ([slot][chunk][thread]) so a warp's 16-byte accesses
 // hit consecutive banks.  Only the owning thread reads its slots, so no
 // block-level barrier is needed.
-template <class F, bool FP64 = false>
+template <class F>
 __global__ void __launch_bounds__(ACC_THREADS) k_accumulate(const uint4 *__restrict__ bases, const uint32_t *__restrict__ entries,
                                                     const uint32_t *__restrict__ offsets, int64_t K, int64_t nthreads,
                                                     xyzz_t<F> *__restrict__ buckets,
                                                     xyzz_t<F> *__restrict__ part_head, xyzz_t<F> *__restrict__ part_tail,
                                                     int32_t *__restrict__ head_key, int32_t *__restrict__ tail_key) {
   using T = typename F::T;
-  using FA = typename AccSel<F, FP64>::type;
+  using FA = typename AccPolicy<F>::type;
   constexpr int CH = F::LIMBS / 2;  // 16-byte chunks of x || y
   extern __shared__ uint4 stage_mem[];  // [2][CH][ACC_THREADS], acc_smem_bytes<F>()
   auto stage = reinterpret_cast<uint4(*)[CH][ACC_THREADS]>(stage_mem);
@@ -635,140 +489,6 @@ __global__ void __launch_bounds__(ACC_THREADS) k_accumulate(const uint4 *__restr
   }
   head_key[t] = hk;
   tail_key[t] = tk;
-}
-
-// 5. the slice that opened a straddling bucket folds in the following slices
-template <class F>
-__global__ void __launch_bounds__(128) k_fixup(const uint32_t *__restrict__ offsets, int64_t K, int64_t nthreads,
-                                               xyzz_t<F> *__restrict__ buckets, const xyzz_t<F> *__restrict__ part_head,
-                                               const xyzz_t<F> *__restrict__ part_tail,
-                                               const int32_t *__restrict__ head_key, const int32_t *__restrict__ tail_key,
-                                               uint32_t *__restrict__ err) {
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= nthreads) return;
-  const int32_t k = tail_key[t];
-  if (k < 0) return;
-  const uint32_t M = __ldg(offsets + K);
-  const uint64_t chunk64 = ((uint64_t)M + nthreads - 1) / nthreads;
-  const uint32_t chunk = chunk64 > 0 ? (uint32_t)chunk64 : 1u;
-  using FA = typename OutOfLine<F>::type;
-  xyzz_t<FA> acc = as_xyzz<FA>(part_tail[t]);
-  const uint64_t bend = __ldg(offsets + k + 1);
-  int64_t t2 = t + 1;
-  while (t2 < nthreads) {
-    if (head_key[t2] != k) {  // cannot happen for a consistent slicing
-      atomicOr(err, 1u);
-      break;
-    }
-    xyzz_add_cold<FA>(acc, as_xyzz<FA>(part_head[t2]));
-    if ((uint64_t)(t2 + 1) * chunk >= bend) break;
-    t2++;
-  }
-  buckets[k] = as_xyzz<F>(acc);
-}
-
-// ---------------------------------------------------------------------------
-// 6. bucket reduction: per window  S = sum_{j=0}^{B-1} (j+1) * V_j.
-//
-// k_reduce_segments: one thread per segment [j0, j0+L) of a window computes,
-// by a running sum from the top, ws = sum (j - j0) V_j and a = sum V_j, then
-// its share of S directly:  ws + (j0 + 1) * a  (double-and-add by the small
-// integer j0 + 1).  The segment shares of a window are then added by a
-// fan-in tree (k_tree_sum).  Serial depth: 2L additions + log2(B) doublings
-// + log_fan(B/L) tree levels, with every stage spread over all segments.
-// ---------------------------------------------------------------------------
-template <class F>
-__global__ void __launch_bounds__(128) k_reduce_segments(const xyzz_t<F> *__restrict__ buckets,
-                                                         const uint32_t *__restrict__ offsets, int W, int B, int L,
-                                                         xyzz_t<F> *__restrict__ V_out) {
-  using FA = typename OutOfLine<F>::type;
-  const int nseg = (B + L - 1) / L;
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (int64_t)W * nseg) return;
-  const int w = (int)(t / nseg), s = (int)(t % nseg);
-  const int64_t kb = (int64_t)w * B;
-  xyzz_t<FA> acc, ws;
-  xyzz_set_inf(acc);
-  xyzz_set_inf(ws);
-  const int j0 = s * L, j1 = min(B, j0 + L);
-  for (int j = j1 - 1; j >= j0; j--) {
-    if (__ldg(offsets + kb + j + 1) != __ldg(offsets + kb + j)) xyzz_add<FA>(acc, as_xyzz<FA>(buckets[kb + j]));
-    if (j > j0) xyzz_add<FA>(ws, acc);
-  }
-  // ws += (j0 + 1) * acc, MSB-first double-and-add
-  const uint32_t mult = (uint32_t)j0 + 1u;
-  if (!xyzz_is_inf(acc)) {
-    xyzz_t<FA> m;
-    xyzz_set_inf(m);
-    for (int b = 31 - __clz(mult); b >= 0; b--) {
-      xyzz_dbl<FA>(m, m);
-      if ((mult >> b) & 1u) xyzz_add<FA>(m, acc);
-    }
-    xyzz_add<FA>(ws, m);
-  }
-  V_out[t] = as_xyzz<F>(ws);
-}
-
-// out[g][i] = sum_{k < fan} in[g][i*fan + k]  (groups of N elements)
-template <class F>
-__global__ void __launch_bounds__(128) k_tree_sum(const xyzz_t<F> *__restrict__ in, int groups, int N, int fan,
-                                                  xyzz_t<F> *__restrict__ out) {
-  using FA = typename OutOfLine<F>::type;
-  const int nout = (N + fan - 1) / fan;
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (int64_t)groups * nout) return;
-  const int g = (int)(t / nout), i = (int)(t % nout);
-  const int64_t base = (int64_t)g * N + (int64_t)i * fan;
-  xyzz_t<FA> acc = as_xyzz<FA>(in[base]);
-  for (int k = 1; k < fan && i * fan + k < N; k++) xyzz_add<FA>(acc, as_xyzz<FA>(in[base + k]));
-  out[t] = as_xyzz<F>(acc);
-}
-
-// 7. Horner over windows on the device, one thread per MSM (used inside
-// CUDA-graph capture and for batches, where the host tail is not used);
-// writes the homogeneous projective result (X, Y, Z; u64 limbs; Montgomery).
-template <class F>
-__global__ void k_combine(const xyzz_t<F> *__restrict__ S, int n_msm, int W, int c, uint64_t *__restrict__ out_proj) {
-  using FA = typename OutOfLine<F>::type;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n_msm) return;
-  xyzz_t<FA> res;
-  xyzz_set_inf(res);
-  for (int w = W - 1; w >= 0; w--) {
-    if (!xyzz_is_inf(res))
-      for (int k = 0; k < c; k++) xyzz_dbl<FA>(res, res);
-    xyzz_add<FA>(res, as_xyzz<FA>(S[(int64_t)i * W + w]));
-  }
-  typename F::T X, Y, Z;
-  xyzz_to_proj<FA>(X, Y, Z, res);
-  constexpr int H = F::LIMBS / 2;  // u64 words per coordinate
-  uint64_t *o = out_proj + (int64_t)i * 3 * H;
-  store_ref<F>(o, X);
-  store_ref<F>(o + H, Y);
-  store_ref<F>(o + 2 * H, Z);
-}
-
-// Horner per MSM of a batch; MSM i writes result slot out_index[i].
-template <class F>
-__global__ void k_combine_indexed(const xyzz_t<F> *__restrict__ S, int n_msm, int W, int c,
-                                  const int32_t *__restrict__ out_index, uint64_t *__restrict__ out_proj) {
-  using FA = typename OutOfLine<F>::type;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n_msm) return;
-  xyzz_t<FA> res;
-  xyzz_set_inf(res);
-  for (int w = W - 1; w >= 0; w--) {
-    if (!xyzz_is_inf(res))
-      for (int k = 0; k < c; k++) xyzz_dbl<FA>(res, res);
-    xyzz_add<FA>(res, as_xyzz<FA>(S[(int64_t)i * W + w]));
-  }
-  typename F::T X, Y, Z;
-  xyzz_to_proj<FA>(X, Y, Z, res);
-  constexpr int H = F::LIMBS / 2;
-  uint64_t *o = out_proj + (int64_t)__ldg(out_index + i) * 3 * H;
-  store_ref<F>(o, X);
-  store_ref<F>(o + H, Y);
-  store_ref<F>(o + 2 * H, Z);
 }
 
 }  // namespace gm

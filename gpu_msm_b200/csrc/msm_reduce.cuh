@@ -242,22 +242,27 @@ struct RedLayout {
   int64_t G = 0;
   int sms = 1, dev = 0;  // device the level-0 grid is sized for
   int B = 0, L0 = 0, nseg0 = 0, L1 = 0, nseg1 = 0, M = 0;
-  static constexpr int FAN = 4;
+  static constexpr int FAN = 2;
   size_t o_X = 0, o_A0 = 0, o_t[2] = {0, 0};
 
   // wave_threads: level-0 threads resident at once on the device.  L0 is at
   // least 16 buckets for G1 and 4 for G2 (an Fp2 addition takes three times
   // as long, so G2 wants shorter chains), and larger when the segments would
-  // not fit one wave.
+  // not fit one wave.  coop_wave: threads of the cooperative level-1 kernel
+  // resident at once (0: no limit); L1 is at least 8 segments, and larger
+  // when the level-1 groups (Coop<F>::LANES threads each) would not fit one
+  // wave: a second wave would double the level's serial time.
   template <class F, class Carver>
-  void plan(int64_t G_, int B_, int64_t wave_threads, Carver &cv) {
+  void plan(int64_t G_, int B_, int64_t wave_threads, Carver &cv, int64_t coop_wave = 0) {
     G = G_;
     B = B_;
     int64_t l0 = sizeof(typename F::T) == sizeof(fp_t) ? 16 : 4;
     if (wave_threads > 0) l0 = std::max<int64_t>(l0, (G * B + wave_threads - 1) / wave_threads);
     L0 = (int)std::min<int64_t>(l0, B);
     nseg0 = (B + L0 - 1) / L0;
-    L1 = nseg0 < 8 ? nseg0 : 8;
+    int64_t l1 = 8;
+    if (coop_wave > 0) l1 = std::max<int64_t>(l1, (G * nseg0 * Coop<F>::LANES + coop_wave - 1) / coop_wave);
+    L1 = (int)std::min<int64_t>(l1, nseg0);
     nseg1 = nseg0 > 1 ? (nseg0 + L1 - 1) / L1 : 0;
     M = nseg0 + nseg1;
     o_X = cv.template take<xyzz_t<F>>((size_t)(G * M));

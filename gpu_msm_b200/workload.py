@@ -17,6 +17,8 @@ import numpy as np
 # u = -0x6008204000000020001 of this curve (p = (u-1)^2 r / 3 + u)
 U_PARAM = -0x6008204000000020001
 R_ORDER = U_PARAM ** 4 - U_PARAM ** 2 + 1
+# base-field prime p = (u - 1)^2 r / 3 + u (446 bits)
+P_MODULUS = (U_PARAM - 1) ** 2 * R_ORDER // 3 + U_PARAM
 R_LIMBS = np.array([(R_ORDER >> (64 * i)) & 0xFFFFFFFFFFFFFFFF for i in range(5)], dtype=np.uint64)
 SCALAR_LIMBS = 5
 SCALAR_BITS = R_ORDER.bit_length()  # 299
@@ -87,6 +89,51 @@ def expected_log(scalars: np.ndarray, logs: np.ndarray) -> int:
     for k, t in zip(ks, ts):
         acc += k * t
     return acc % R_ORDER
+
+
+def limbs16(a: np.ndarray) -> np.ndarray:
+    """(n, L) little-endian u64 limbs -> (n, 4L) float64 array of their
+    16-bit limbs (each an exact integer below 2^16)."""
+    a = np.ascontiguousarray(a, dtype=np.uint64)
+    return a.view(np.uint16).reshape(len(a), -1).astype(np.float64)
+
+
+# rows per exact product chunk: n (2^16 - 1)^2 < 2^53 keeps every partial sum
+# of the float64 matrix product an exact integer
+_DOT_CHUNK = 1 << 20
+
+
+def dot_log(k16: np.ndarray, t16: np.ndarray) -> int:
+    """sum_i k_i t_i mod r from 16-bit limb rows (limbs16): the limb-product
+    sums sum_i k_i[a] t_i[b] are computed exactly as float64 matrix products
+    over chunks of at most 2^20 rows, then weighted by 2^(16 (a + b))."""
+    n = len(k16)
+    if n != len(t16):
+        raise ValueError("scalars and logs must have the same number of rows")
+    acc = 0
+    for r0 in range(0, n, _DOT_CHUNK):
+        m = (k16[r0:r0 + _DOT_CHUNK].T @ t16[r0:r0 + _DOT_CHUNK]).astype(np.int64)
+        la, lb = m.shape
+        for c in range(la + lb - 1):
+            a0, a1 = max(0, c - lb + 1), min(la - 1, c)
+            s = int(sum(int(m[a, c - a]) for a in range(a0, a1 + 1)))
+            acc += s << (16 * c)
+    return acc % R_ORDER
+
+
+def expected_logs(sizes, scalars: np.ndarray, logs: np.ndarray, base_offsets=None) -> list:
+    """Discrete logs of the exact results of consecutive MSMs: MSM j takes the
+    next sizes[j] scalar rows and the logs [base_offsets[j], + sizes[j]) of
+    the table (prefixes when base_offsets is None)."""
+    k16 = limbs16(scalars)
+    t16 = limbs16(logs)
+    out, row = [], 0
+    for j, s in enumerate(np.asarray(sizes, dtype=np.int64)):
+        s = int(s)
+        o = 0 if base_offsets is None else int(base_offsets[j])
+        out.append(dot_log(k16[row:row + s], t16[o:o + s]))
+        row += s
+    return out
 
 
 def int_to_limbs(v: int, n: int = 5) -> np.ndarray:

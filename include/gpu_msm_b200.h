@@ -150,9 +150,13 @@ int gm_g2_msm_device_affine(gm_stream_t stream, uint32_t gpu_index, G2Point *d_r
  * 1 <= scalar_limbs <= 8; larger requests return -1 without launching.  All
  * calls share the array: calls that overlap on the GPU race, so order them on
  * one stream.  The first call on a device looks up the array's address on
- * that device; make it before any stream capture there. */
+ * that device; make it before any stream capture there.  d_err (device
+ * pointer, may be NULL) receives, on the stream, the pipeline's consistency
+ * flag: 0, or non-zero if the result must not be trusted (the regular
+ * blocking wrappers return -5 in that case). */
 int gm_g1_msm_device_noalloc(gm_stream_t stream, uint32_t gpu_index, G1ProjectivePoint *d_result,
-                             const G1Point *d_points, const uint64_t *d_scalars, int scalar_limbs, int n);
+                             const G1Point *d_points, const uint64_t *d_scalars, int scalar_limbs, int n,
+                             uint32_t *d_err);
 
 /* Resident base tables and batched MSMs.  No reference counterpart: every
  * reference MSM copies and converts its bases again (c_wrapper.cu:64-172).
@@ -369,26 +373,13 @@ int gm_g1_sum_projective_host(G1ProjectivePoint *out, const G1ProjectivePoint *i
  *   calling thread since the previous call.
  * gm_imad_probe: launches a kernel of independent multiply-add chains over
  *   the whole GPU (mode 0: half mad.lo, half mad.hi, the mix of an integer
- *   Montgomery product; mode 1: mad.lo only; mode 2: fma.rn.f64, the pipe of
- *   the FP64 Montgomery product); *imad_per_launch receives the instruction
+ *   Montgomery product; mode 1: mad.lo only); *imad_per_launch receives the instruction
  *   count so that the caller can time it and derive the ceiling. */
 int gm_profile_enable(int on);
 int gm_profile_collect(char *names, int names_len, float *ms, int max);
 int64_t gm_launch_count_reset(void);
 int gm_imad_probe(gm_stream_t stream, uint32_t gpu_index, int iters, int mode, uint32_t *d_sink,
                   int64_t sink_words, int64_t *imad_per_launch);
-
-/* Product mode of the G1 bucket accumulation (no reference counterpart).
- * 0 (default): the integer CIOS Montgomery product on the IMAD pipe.
- * 1: the same function computed on the FP64 pipe -- 52-bit limbs split
- *    exactly by fma.rz.f64 and integer column sums, every intermediate an
- *    exact integer and every result bit-identical to mode 0 -- which runs the
- *    G1 2^20 accumulation in 11.1 ms instead of 13.3 ms on B200.
- * The initial mode comes from the environment variable GM_FP64_PRODUCTS
- * (1 = on).  The mode is read when an MSM (or a batch plan) is launched or
- * created; G2 always uses the integer product. */
-int gm_set_fp64_products(int on);
-int gm_fp64_products(void);
 
 /* Last CUDA error string seen by this library on the calling thread. */
 const char *gm_last_error(void);

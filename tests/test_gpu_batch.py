@@ -205,19 +205,73 @@ def test_batch_precomputed_g2(cuda):
     check(res, expected(sizes, offs, sc, logs, 2), 2)
 
 
-def test_batch_fp64_products_mode(cuda):
-    """Batch plans made in the FP64-product mode (G1 accumulation products on
-    the FP64 pipe), with and without window tables, equal the oracle."""
+def _generator_multiples(logs_list, group):
+    """(s mod r) * G for every s, from the oracle, in parallel (the oracle's C
+    calls release the GIL)."""
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=8) as ex:
+        return list(ex.map(lambda s: oracle.generator_multiple(s, group=group), logs_list))
+
+
+def _check_all(res_t, sizes, sc, logs, group=1):
+    want = _generator_multiples(wl.expected_logs(sizes, sc, logs), group)
+    got = gm.to_numpy_proj(res_t, group)
+    bad = [i for i, w in enumerate(want) if not oracle.same_point(oracle.proj_to_affine(got[i:i + 1], group), w)]
+    assert not bad, f"{len(bad)} of {len(want)} outputs differ, first {bad[:5]}"
+
+
+def test_batch_512_config_every_output(cuda):
+    """The batched benchmark configuration exactly: 512 G1 MSMs of sizes
+    floor(2^U), U ~ U[8, 16] (seed 7), each with its own scalars over a prefix
+    of one resident 2^16-point table; window widths from the autotuner's
+    table; the plan captured in a CUDA graph and replayed.  Every one of the
+    512 outputs equals (sum_i k_i t_i mod r) * G, on two replays with
+    different scalars, without and with fixed-base window tables."""
     import torch
-    gm.set_fp64_products(True)
-    try:
-        table, logs = make_table(1 << 11, 1, cuda, seed=171)
-        table.precompute(8)
-        sizes, offs, sc = batch_inputs(1 << 11, 24, 1, 11, seed=172)
-        wins = np.array([[5, 8][i % 2] for i in range(len(sizes))], dtype=np.int32)
-        plan = gm.BatchPlan(table, sizes, offs, window_bits=wins)
-        res = plan.run(t_dev(sc, cuda).reshape(-1, 5))
+    n_table, count = 1 << 16, 512
+    table, logs = make_table(n_table, 1, cuda, seed=7070)
+    sizes = wl.mixed_sizes(count, 8, 16, seed=7)
+    total = int(sizes.sum())
+    static_sc = torch.empty((total, 5), dtype=torch.int64, device=cuda)
+    out = torch.empty((count, gm.G1P_WORDS), dtype=torch.int64, device=cuda)
+
+    def graph_of(plan):
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            plan.run(static_sc, out=out)
+        torch.cuda.current_stream().wait_stream(s)
         torch.cuda.synchronize()
-        check(res, expected(sizes, offs, sc, logs, 1), 1)
-    finally:
-        gm.set_fp64_products(False)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, capture_error_mode="thread_local"):
+            plan.run(static_sc, out=out)
+        return g
+
+    sc0 = wl.make_scalars(total, seed=7171)
+    static_sc.copy_(t_dev(sc0, cuda).reshape(-1, 5))
+    plan = gm.BatchPlan(table, sizes)
+    assert len(plan.classes()) > 1
+    g = graph_of(plan)
+    for seed in (7171, 7272):
+        sc = wl.make_scalars(total, seed=seed)
+        static_sc.copy_(t_dev(sc, cuda).reshape(-1, 5))
+        out.zero_()
+        g.replay()
+        torch.cuda.synchronize()
+        _check_all(out, sizes, sc, logs)
+    del g
+    plan.close()
+    for c in (8, 10, 12, 14, 16):
+        table.precompute(c)
+    plan = gm.BatchPlan(table, sizes)
+    g = graph_of(plan)
+    for seed in (7373, 7474):
+        sc = wl.make_scalars(total, seed=seed)
+        static_sc.copy_(t_dev(sc, cuda).reshape(-1, 5))
+        out.zero_()
+        g.replay()
+        torch.cuda.synchronize()
+        _check_all(out, sizes, sc, logs)
+    del g
+    plan.close()
+    table.close()

@@ -81,11 +81,10 @@ def test_fp_edges(cuda):
 
 
 def test_fp_mont_mul_limb52_patterns(cuda):
-    """The FP64-pipe product works on 52-bit limbs: operands whose 52-bit
-    limbs sit at the split boundaries (all ones, zero, single high bits,
-    values just below p in each limb position) against the oracle, both
-    orders, bit-exact; also the G1 accumulation path's out-of-line product
-    through a full MSM is covered by the MSM tests."""
+    """Structured operands: runs of ones, single high bits and values just
+    below p at 52-bit strides (boundaries that do not line up with the 32-bit
+    limbs of the product), against the oracle and the exact integer product,
+    both orders, bit-exact."""
     P = pyref.P
     M = (1 << 52) - 1
     pats = [0, 1, M, 1 << 51, (1 << 52) - 2, P - 1, P - 2, P >> 1, (P + 1) // 2]

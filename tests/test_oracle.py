@@ -18,6 +18,7 @@ import pytest
 
 import oracle
 from oracle import pyref
+from gpu_msm_b200 import workload as wl
 
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
 
@@ -195,3 +196,21 @@ def test_cpu_config_pippenger_equals_naive():
     assert oracle.same_point(a, b)
     c = oracle.generator_multiple(workload.expected_log(sc, logs))
     assert oracle.same_point(a, c)
+
+
+def test_fast_expected_log_matches_big_integers():
+    """workload.dot_log (exact float64 limb-product sums) equals the plain
+    big-integer sum_i k_i t_i mod r, for 1, 5 and 8 limbs and across the
+    2^20-row chunk boundary."""
+    rng = np.random.default_rng(3)
+    for n, limbs in [(1, 5), (33, 1), (2000, 8), ((1 << 20) + 3, 5)]:
+        sc = rng.integers(0, 2 ** 64, size=(n, limbs), dtype=np.uint64)
+        logs = wl.make_base_logs(n, seed=n)
+        assert wl.dot_log(wl.limbs16(sc), wl.limbs16(logs)) == wl.expected_log(sc, logs)
+    sizes = np.array([5, 1, 300], dtype=np.int64)
+    sc = wl.make_scalars(306, seed=4)
+    logs = wl.make_base_logs(400, seed=5)
+    offs = np.array([0, 7, 100])
+    got = wl.expected_logs(sizes, sc, logs, offs)
+    assert got == [wl.expected_log(sc[0:5], logs[0:5]), wl.expected_log(sc[5:6], logs[7:8]),
+                   wl.expected_log(sc[6:306], logs[100:400])]
