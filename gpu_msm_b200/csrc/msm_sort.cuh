@@ -15,8 +15,9 @@
 // counts its tile's entries per (group, hi) with shared-memory atomics
 // (k_sort_a_count), one exclusive scan over the count matrix
 // [group][hi][tile] gives every (group, hi, tile) its output range, and the
-// same block recomputes the digits and writes each entry at its range start
-// plus its rank inside the tile (k_sort_a_scatter).  Ranks come from
+// same block reads the digits back (the counting kernel stores them) and
+// writes each entry at its range start plus its rank inside the tile
+// (k_sort_a_scatter).  Ranks come from
 // per-warp counters and a ballot per digit bit over 32 consecutive points,
 // so the order inside a (group, hi) range is the point order.
 // Pass B (only when c - 1 > 8 bits) sorts every (group, hi) segment by
@@ -121,16 +122,15 @@ GM_DEVI uint32_t lanemask_lt() {
   return m;
 }
 
-// Lanes of the warp holding the same bin (a bits-wide value), by one ballot
+// Lanes of the warp holding the same bin (a BITS-wide value), by one ballot
 // per bit; only meaningful for lanes with valid set.
-GM_DEVI uint32_t same_bin_lanes(uint32_t bin, bool valid, int bits) {
+template <int BITS>
+GM_DEVI uint32_t same_bin_lanes(uint32_t bin, bool valid) {
   uint32_t peers = __ballot_sync(0xffffffffu, valid);
 #pragma unroll
-  for (int k = 0; k < 12; k++) {
-    if (k >= bits) break;
-    const bool set = (bin >> k) & 1u;
-    const uint32_t b = __ballot_sync(0xffffffffu, set);
-    peers &= set ? b : ~b;
+  for (int k = 0; k < BITS; k++) {
+    const uint32_t b = __ballot_sync(0xffffffffu, (bin >> k) & 1u);
+    peers &= ((bin >> k) & 1u) ? b : ~b;
   }
   return peers;
 }
@@ -152,24 +152,31 @@ GM_DEVI int signed_digit(const uint64_t *s, int limbs, int w, const DigitParams 
   return (int)raw;
 }
 
-// Windows per chunk of the pass-A scatter: the chunk's digits are kept in
-// shared memory between its counting and ranking sweeps, and its per-warp
-// counters are [SORT_WARPS][chunk groups][RA].
+// Windows per chunk of the pass-A scatter: its per-warp counters are
+// [SORT_WARPS][chunk groups][RA].
 constexpr int SA_CHUNK_W = 4;
 __host__ __device__ inline int sort_a_chunk(const SortParams &sp) { return sp.dp.W < SA_CHUNK_W ? sp.dp.W : SA_CHUNK_W; }
 // counter groups of one chunk: its windows, or the one group of the
 // fixed-base table mode
 __host__ __device__ inline int sort_a_groups(const SortParams &sp) { return sp.S == 1 ? 1 : sort_a_chunk(sp); }
-
-// Dynamic shared memory of k_sort_a_*: staged scalars, then the counters
-// ([S][RA] for counting; for the scatter [SORT_WARPS][groups][RA], a
-// running count per hi, and the signed digits of one chunk).
-inline size_t sort_a_smem(const SortParams &sp, bool scatter) {
-  const size_t sc = (size_t)SA_TP * sp.dp.limbs * sizeof(uint64_t);
-  if (!scatter) return sc + (size_t)sp.S * sp.RA * sizeof(uint32_t);
-  const size_t GR = (size_t)sort_a_groups(sp) * sp.RA;
-  return sc + (SORT_WARPS * GR + sp.RA) * sizeof(uint32_t) + (size_t)sort_a_chunk(sp) * SA_TP * sizeof(int32_t);
+// scatter blocks per pass-A tile: one per chunk, or one for the single group
+// (whose chunks depend on each other's counts)
+__host__ __device__ inline int sort_a_blocks_per_tile(const SortParams &sp) {
+  return sp.S == 1 ? 1 : (sp.dp.W + sort_a_chunk(sp) - 1) / sort_a_chunk(sp);
 }
+
+// Dynamic shared memory of k_sort_a_*: for counting, the staged scalars and
+// the counters [S][RA]; for the scatter, the per-warp counters
+// [SORT_WARPS][groups][RA] and a running count per hi.
+inline size_t sort_a_smem(const SortParams &sp, bool scatter) {
+  if (!scatter) return (size_t)SA_TP * sp.dp.limbs * sizeof(uint64_t) + (size_t)sp.S * sp.RA * sizeof(uint32_t);
+  const size_t GR = (size_t)sort_a_groups(sp) * sp.RA;
+  return (SORT_WARPS * GR + sp.RA) * sizeof(uint32_t);
+}
+
+// Signed digits of the pass-A tiles, written by the counting kernel and read
+// by the scatter: dig[(tile * W + w) * SA_TP + q] for point slot q.
+GM_DEVI int64_t dig_index(int tile, int W, int w, int q) { return ((int64_t)tile * W + w) * SA_TP + q; }
 
 // Digits of the tile's points for windows [w0, w1), in (warp, round, lane)
 // order: warp wp takes points [32 SA_PPT wp, 32 SA_PPT (wp + 1)), 32 per
@@ -198,12 +205,14 @@ GM_DEVI void stage_scalars(uint64_t *sc, const uint64_t *scalars, const TileA &t
   for (int64_t k = threadIdx.x; k < words; k += SA_THREADS) sc[k] = __ldg(src + k);
 }
 
-// Pass A, counting: the tile's entries per (group in MSM, hi digit) with
-// shared-memory atomics; writes every counter of the tile.
+// Pass A, counting: the tile's signed digits (into dig) and its entries per
+// (group in MSM, hi digit), counted with shared-memory atomics; writes every
+// counter of the tile.
 static __global__ void __launch_bounds__(SA_THREADS) k_sort_a_count(const uint64_t *__restrict__ scalars, SortDesc sd,
-                                                                  SortParams sp, uint32_t *__restrict__ cnt) {
+                                                                  SortParams sp, uint32_t *__restrict__ cnt,
+                                                                  int32_t *__restrict__ dig) {
   extern __shared__ uint64_t sort_smem[];
-  const int limbs = sp.dp.limbs, RA = sp.RA, SR = sp.S * RA;
+  const int limbs = sp.dp.limbs, RA = sp.RA, SR = sp.S * RA, W = sp.dp.W;
   uint64_t *sc = sort_smem;
   uint32_t *h = reinterpret_cast<uint32_t *>(sc + (size_t)SA_TP * limbs);  // [S][RA]
   const TileA ti = tile_a_info(sd, sp, blockIdx.x);
@@ -212,7 +221,8 @@ static __global__ void __launch_bounds__(SA_THREADS) k_sort_a_count(const uint64
   __syncthreads();
   const int shift = sp.passes == 2 ? sp.LB : 0;
   uint32_t carry[SA_PPT] = {0};
-  tile_digits(sc, ti, sp, 0, sp.dp.W, carry, [&](int w, int, int d) {
+  tile_digits(sc, ti, sp, 0, W, carry, [&](int w, int q, int d) {
+    dig[dig_index(blockIdx.x, W, w, q)] = d;
     if (d == 0) return;
     const uint32_t b = (uint32_t)(d < 0 ? -d : d) - 1u;
     atomicAdd(&h[(sp.S == 1 ? 0 : w) * RA + (b >> shift)], 1u);
@@ -221,42 +231,54 @@ static __global__ void __launch_bounds__(SA_THREADS) k_sort_a_count(const uint64
   for (int k = threadIdx.x; k < SR; k += SA_THREADS) cnt[idx_a(ti, sp, k / RA, k % RA, ti.t)] = h[k];
 }
 
-// Pass A, scatter: cnt holds the scanned count matrix.  Windows go in chunks
-// of sort_a_chunk; per chunk: the signed digits (kept in shared memory) and
-// the per-warp counts of every (group, hi); their exclusive prefix over the
-// warps on top of the tile's output range (and, with one group, of the
-// earlier chunks' entries); then every entry at its warp's running position
-// plus its rank among the warp's lanes.  Two passes: (key b, value) pairs
-// into kv; one pass: values into entries (final order).
-static __global__ void __launch_bounds__(SA_THREADS) k_sort_a_scatter(const uint64_t *__restrict__ scalars, SortDesc sd,
+// Pass A, scatter: cnt holds the scanned count matrix, dig the tile's
+// digits.  Windows go in chunks of sort_a_chunk; per chunk: the per-warp
+// counts of every (group, hi); their exclusive prefix over the warps on top
+// of the tile's output range (and, with one group, of the earlier chunks'
+// entries); then every entry at its warp's running position plus its rank
+// among the warp's lanes.  Two passes: (key b, value) pairs into kv; one
+// pass: values into entries (final order).  HB: bits of the hi digit.
+template <int HB>
+__global__ void __launch_bounds__(SA_THREADS) k_sort_a_scatter(const int32_t *__restrict__ dig, SortDesc sd,
                                                                     SortParams sp, const uint32_t *__restrict__ cnt,
                                                                     uint2 *__restrict__ kv,
                                                                     uint32_t *__restrict__ entries) {
-  extern __shared__ uint64_t sort_smem[];
-  const int limbs = sp.dp.limbs, RA = sp.RA;
+  extern __shared__ uint32_t sa_smem[];
+  const int RA = sp.RA, W = sp.dp.W;
   const int WC = sort_a_chunk(sp);
   const int GR = sort_a_groups(sp) * RA;
-  uint64_t *sc = sort_smem;
-  uint32_t *wc = reinterpret_cast<uint32_t *>(sc + (size_t)SA_TP * limbs);  // [SORT_WARPS][GR]
-  uint32_t *run = wc + SORT_WARPS * GR;                                     // [RA] earlier chunks (one group)
-  int32_t *dg = reinterpret_cast<int32_t *>(run + RA);                      // [WC][SA_TP] digits
-  const int warp = threadIdx.x >> 5;
+  uint32_t *wc = sa_smem;                 // [SORT_WARPS][GR]
+  uint32_t *run = wc + SORT_WARPS * GR;   // [RA] earlier chunks (one group)
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint32_t *my = wc + warp * GR;
-  const TileA ti = tile_a_info(sd, sp, blockIdx.x);
-  stage_scalars(sc, scalars, ti, limbs);
+  // one block per (tile, chunk) with one group per window; one block per
+  // tile (all chunks, in order) with the single group of table mode
+  const int nch = sort_a_blocks_per_tile(sp);
+  const int tile = blockIdx.x / nch;
+  const int wbeg = sp.S == 1 ? 0 : (blockIdx.x % nch) * WC;
+  const int wend = sp.S == 1 ? W : min(W, wbeg + WC);
+  const TileA ti = tile_a_info(sd, sp, tile);
   for (int k = threadIdx.x; k < RA; k += SA_THREADS) run[k] = 0;
   const int shift = sp.passes == 2 ? sp.LB : 0;
-  uint32_t carry[SA_PPT] = {0};
-  for (int w0 = 0; w0 < sp.dp.W; w0 += WC) {
-    const int w1 = min(sp.dp.W, w0 + WC);
+  for (int w0 = wbeg; w0 < wend; w0 += WC) {
+    const int w1 = min(W, w0 + WC);
     for (int k = threadIdx.x; k < SORT_WARPS * GR; k += SA_THREADS) wc[k] = 0;
     __syncthreads();
-    tile_digits(sc, ti, sp, w0, w1, carry, [&](int w, int q, int d) {
-      dg[(w - w0) * SA_TP + q] = d;
-      if (d == 0) return;
-      const uint32_t b = (uint32_t)(d < 0 ? -d : d) - 1u;
-      atomicAdd(&my[(sp.S == 1 ? 0 : w - w0) * RA + (b >> shift)], 1u);
-    });
+    int dg[SA_CHUNK_W][SA_PPT];
+#pragma unroll
+    for (int j = 0; j < SA_CHUNK_W; j++) {
+      const int w = w0 + j;
+#pragma unroll
+      for (int r = 0; r < SA_PPT; r++) {
+        const int q = warp * (32 * SA_PPT) + r * 32 + lane;
+        dg[j][r] = (w < w1 && q < ti.np) ? __ldg(dig + dig_index(tile, W, w, q)) : 0;
+        if (dg[j][r] != 0) {
+          const int d = dg[j][r];
+          const uint32_t b = (uint32_t)(d < 0 ? -d : d) - 1u;
+          atomicAdd(&my[(sp.S == 1 ? 0 : j) * RA + (b >> shift)], 1u);
+        }
+      }
+    }
     __syncthreads();
     // running position of every (warp, group, hi) of the chunk: the tile's
     // range start plus the entries of the lower warps (and earlier chunks)
@@ -273,21 +295,26 @@ static __global__ void __launch_bounds__(SA_THREADS) k_sort_a_scatter(const uint
       if (sp.S == 1) run[d] = acc - base;
     }
     __syncthreads();
-    const int lane = threadIdx.x & 31;
-    for (int w = w0; w < w1; w++) {
+    const uint32_t rbase = (uint32_t)ti.base_off;
+#pragma unroll
+    for (int j = 0; j < SA_CHUNK_W; j++) {
+      const int w = w0 + j;
+      if (w >= w1) break;
+      const uint32_t wofs = sd.pc_stride ? (uint32_t)((int64_t)w * sd.pc_stride) : 0u;
 #pragma unroll
       for (int r = 0; r < SA_PPT; r++) {
         const int q = warp * (32 * SA_PPT) + r * 32 + lane;
-        const int d = q < ti.np ? dg[(w - w0) * SA_TP + q] : 0;
+        const int d = dg[j][r];
         const uint32_t b = (uint32_t)(d < 0 ? -d : d) - 1u;
         const uint32_t bin = d != 0 ? (b >> shift) : 0u;
-        const uint32_t peers = same_bin_lanes(bin, d != 0, sp.HB);
+        const uint32_t peers = same_bin_lanes<HB>(bin, d != 0);
         if (d != 0) {
-          uint32_t *slot = &my[(sp.S == 1 ? 0 : w - w0) * RA + bin];
+          uint32_t *slot = &my[(sp.S == 1 ? 0 : j) * RA + bin];
           const uint32_t lower = peers & lanemask_lt();
           const uint32_t pos = *slot + __popc(lower);
-          const int64_t rec = (sd.pc_stride ? (int64_t)w * sd.pc_stride : 0) + ti.base_off + q;
-          const uint32_t val = ((uint32_t)rec << 1) | (d < 0 ? 1u : 0u);
+          // record index < 2^31: 32-bit arithmetic
+          const uint32_t rec = wofs + rbase + (uint32_t)q;
+          const uint32_t val = (rec << 1) | (d < 0 ? 1u : 0u);
           if (sp.passes == 2)
             kv[pos] = make_uint2(b, val);
           else
@@ -389,7 +416,8 @@ static __global__ void __launch_bounds__(SB_THREADS) k_sort_b_count(const uint2 
 // ranked by lo (per-warp counts, their prefix over warps, lane ranks by
 // ballots) into a shared-memory copy ordered by lo, which is then written
 // out as contiguous runs.
-static __global__ void __launch_bounds__(SB_THREADS) k_sort_b_scatter(const uint2 *__restrict__ kv, SortParams sp,
+template <int LB>
+__global__ void __launch_bounds__(SB_THREADS) k_sort_b_scatter(const uint2 *__restrict__ kv, SortParams sp,
                                                              const uint32_t *__restrict__ seg,
                                                              const uint32_t *__restrict__ tb,
                                                              const uint32_t *__restrict__ cnt,
@@ -445,7 +473,7 @@ static __global__ void __launch_bounds__(SB_THREADS) k_sort_b_scatter(const uint
 #pragma unroll
   for (int r = 0; r < SB_IPT; r++) {
     const bool valid = bin[r] != 0xffffffffu;
-    const uint32_t peers = same_bin_lanes(valid ? bin[r] : 0u, valid, sp.LB);
+    const uint32_t peers = same_bin_lanes<LB>(valid ? bin[r] : 0u, valid);
     if (valid) {
       const int q = warp * (32 * SB_IPT) + r * 32 + lane;
       const uint32_t lower = peers & lanemask_lt();
@@ -492,7 +520,7 @@ static __global__ void k_sort_offsets(SortDesc sd, SortParams sp, int64_t K, con
 struct SortLayout {
   SortParams sp;
   int64_t G = 0, maxM = 0;
-  size_t o_cntA = 0, o_bsA = 0, o_kv = 0, o_seg = 0, o_tb = 0, o_bsT = 0, o_cntB = 0, o_bsB = 0;
+  size_t o_cntA = 0, o_bsA = 0, o_dig = 0, o_kv = 0, o_seg = 0, o_tb = 0, o_bsT = 0, o_cntB = 0, o_bsB = 0;
 
   static int64_t scan_blocks(int64_t len) { return std::max<int64_t>(1, (len + SCAN_TILE - 1) / SCAN_TILE); }
 
@@ -521,6 +549,7 @@ struct SortLayout {
     sp.lenA = (int64_t)sp.S * sp.RA * tilesA;
     maxM = P * dp.W;
     o_cntA = cv.template take<uint32_t>((size_t)sp.lenA + 1);
+    o_dig = cv.template take<int32_t>((size_t)tilesA * dp.W * SA_TP);
     o_bsA = cv.template take<uint32_t>((size_t)scan_blocks(sp.lenA));
     if (sp.passes == 2) {
       sp.tilesB_max = sp.NS + (maxM + SB_TILE - 1) / SB_TILE;
@@ -544,29 +573,73 @@ inline void scan_inplace(cudaStream_t s, uint32_t *a, int64_t len, uint32_t *bsu
   *launches += 3;
 }
 
-// Opt-in shared-memory sizes of the sort kernels: raised on the current
-// device whenever a launch needs more than the largest size set so far.
-inline cudaError_t sort_set_smem_limits(const SortParams &sp) {
+// Raises the opt-in shared-memory size of kernel fn on the current device
+// when a launch needs more than 48 KB and more than the largest size set so
+// far (slot: one per kernel instantiation).
+inline cudaError_t smem_opt_in(const void *fn, int slot, size_t bytes) {
   static std::mutex mu;
-  static int set[64][4] = {{0}};
+  static int set[64][32] = {{0}};
+  if (bytes <= 48 * 1024) return cudaSuccess;
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= 64) dev = 0;
-  const void *fns[4] = {(const void *)k_sort_a_count, (const void *)k_sort_a_scatter, (const void *)k_sort_b_count,
-                        (const void *)k_sort_b_scatter};
-  const int need[4] = {(int)sort_a_smem(sp, false), (int)sort_a_smem(sp, true),
-                       sp.passes == 2 ? (int)sort_b_smem(sp, false) : 0,
-                       sp.passes == 2 ? (int)sort_b_smem(sp, true) : 0};
   std::lock_guard<std::mutex> lk(mu);
-  for (int k = 0; k < 4; k++) {
-    if (need[k] > 48 * 1024 && need[k] > set[dev][k]) {
-      e = cudaFuncSetAttribute(fns[k], cudaFuncAttributeMaxDynamicSharedMemorySize, need[k]);
-      if (e != cudaSuccess) return e;
-      set[dev][k] = need[k];
-    }
-  }
+  if ((int)bytes <= set[dev][slot]) return cudaSuccess;
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) set[dev][slot] = (int)bytes;
+  return e;
+}
+
+template <int HB>
+cudaError_t launch_sort_a_scatter(cudaStream_t s, const SortParams &sp, const int32_t *dig, const SortDesc &sd,
+                                  const uint32_t *cntA, uint2 *kv, uint32_t *entries) {
+  const size_t sm = sort_a_smem(sp, true);
+  cudaError_t e = smem_opt_in((const void *)k_sort_a_scatter<HB>, HB, sm);
+  if (e != cudaSuccess) return e;
+  k_sort_a_scatter<HB><<<(unsigned)(sp.tilesA * sort_a_blocks_per_tile(sp)), SA_THREADS, sm, s>>>(dig, sd, sp, cntA,
+                                                                                             kv, entries);
   return cudaSuccess;
+}
+
+template <int LB>
+cudaError_t launch_sort_b_scatter(cudaStream_t s, const SortParams &sp, const uint2 *kv, const uint32_t *seg,
+                                  const uint32_t *tb, const uint32_t *cntB, uint32_t *entries) {
+  const size_t sm = sort_b_smem(sp, true);
+  cudaError_t e = smem_opt_in((const void *)k_sort_b_scatter<LB>, 16 + LB, sm);
+  if (e != cudaSuccess) return e;
+  k_sort_b_scatter<LB><<<(unsigned)sp.tilesB_max, SB_THREADS, sm, s>>>(kv, sp, seg, tb, cntB, entries);
+  return cudaSuccess;
+}
+
+// The scatters for the digit widths of SortLayout::plan: HB in 1..8 (pass
+// A), LB in 5..11 (pass B).
+inline cudaError_t sort_a_scatter(cudaStream_t s, const SortParams &sp, const int32_t *dig, const SortDesc &sd,
+                                  const uint32_t *cntA, uint2 *kv, uint32_t *entries) {
+  switch (sp.HB) {
+    case 1: return launch_sort_a_scatter<1>(s, sp, dig, sd, cntA, kv, entries);
+    case 2: return launch_sort_a_scatter<2>(s, sp, dig, sd, cntA, kv, entries);
+    case 3: return launch_sort_a_scatter<3>(s, sp, dig, sd, cntA, kv, entries);
+    case 4: return launch_sort_a_scatter<4>(s, sp, dig, sd, cntA, kv, entries);
+    case 5: return launch_sort_a_scatter<5>(s, sp, dig, sd, cntA, kv, entries);
+    case 6: return launch_sort_a_scatter<6>(s, sp, dig, sd, cntA, kv, entries);
+    case 7: return launch_sort_a_scatter<7>(s, sp, dig, sd, cntA, kv, entries);
+    case 8: return launch_sort_a_scatter<8>(s, sp, dig, sd, cntA, kv, entries);
+    default: return cudaErrorInvalidValue;
+  }
+}
+inline cudaError_t sort_b_scatter(cudaStream_t s, const SortParams &sp, const uint2 *kv, const uint32_t *seg,
+                                  const uint32_t *tb, const uint32_t *cntB, uint32_t *entries) {
+  switch (sp.LB) {
+    case 5: return launch_sort_b_scatter<5>(s, sp, kv, seg, tb, cntB, entries);
+    case 6: return launch_sort_b_scatter<6>(s, sp, kv, seg, tb, cntB, entries);
+    case 7: return launch_sort_b_scatter<7>(s, sp, kv, seg, tb, cntB, entries);
+    case 8: return launch_sort_b_scatter<8>(s, sp, kv, seg, tb, cntB, entries);
+    case 9: return launch_sort_b_scatter<9>(s, sp, kv, seg, tb, cntB, entries);
+    case 10: return launch_sort_b_scatter<10>(s, sp, kv, seg, tb, cntB, entries);
+    case 11: return launch_sort_b_scatter<11>(s, sp, kv, seg, tb, cntB, entries);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 // Enqueues the sort: entries[0, M) grouped by bucket key in point order and
@@ -574,31 +647,34 @@ inline cudaError_t sort_set_smem_limits(const SortParams &sp) {
 inline cudaError_t sort_launch(cudaStream_t s, const SortLayout &L, char *ws, const uint64_t *scalars,
                                const SortDesc &sd, int64_t K, uint32_t *offsets, uint32_t *entries, int *launches) {
   const SortParams &sp = L.sp;
-  cudaError_t e = sort_set_smem_limits(sp);
+  cudaError_t e = smem_opt_in((const void *)k_sort_a_count, 0, sort_a_smem(sp, false));
+  if (e == cudaSuccess) e = smem_opt_in((const void *)k_sort_b_count, 9, sort_b_smem(sp, false));
   if (e != cudaSuccess) return e;
   auto *cntA = (uint32_t *)(ws + L.o_cntA);
   auto *bsA = (uint32_t *)(ws + L.o_bsA);
-  k_sort_a_count<<<(unsigned)sp.tilesA, SA_THREADS, sort_a_smem(sp, false), s>>>(scalars, sd, sp, cntA);
+  auto *dig = (int32_t *)(ws + L.o_dig);
+  k_sort_a_count<<<(unsigned)sp.tilesA, SA_THREADS, sort_a_smem(sp, false), s>>>(scalars, sd, sp, cntA, dig);
   scan_inplace(s, cntA, sp.lenA, bsA, launches);
   uint32_t *seg = nullptr, *tb = nullptr, *cntB = nullptr;
-  const size_t smA = sort_a_smem(sp, true);
   if (sp.passes == 1) {
-    k_sort_a_scatter<<<(unsigned)sp.tilesA, SA_THREADS, smA, s>>>(scalars, sd, sp, cntA, nullptr, entries);
+    e = sort_a_scatter(s, sp, dig, sd, cntA, nullptr, entries);
+    if (e != cudaSuccess) return e;
     *launches += 2;
   } else {
     auto *kv = (uint2 *)(ws + L.o_kv);
     seg = (uint32_t *)(ws + L.o_seg);
     tb = (uint32_t *)(ws + L.o_tb);
     cntB = (uint32_t *)(ws + L.o_cntB);
-    k_sort_a_scatter<<<(unsigned)sp.tilesA, SA_THREADS, smA, s>>>(scalars, sd, sp, cntA, kv, nullptr);
+    e = sort_a_scatter(s, sp, dig, sd, cntA, kv, nullptr);
+    if (e != cudaSuccess) return e;
     k_sort_segments<<<(unsigned)((sp.NS + 1 + 255) / 256), 256, 0, s>>>(sd, sp, cntA, seg, tb);
     scan_inplace(s, tb, sp.NS, (uint32_t *)(ws + L.o_bsT), launches);
     e = cudaMemsetAsync(cntB, 0, (size_t)sp.lenB * sizeof(uint32_t), s);
     if (e != cudaSuccess) return e;
     k_sort_b_count<<<(unsigned)sp.tilesB_max, SB_THREADS, sort_b_smem(sp, false), s>>>(kv, sp, seg, tb, cntB);
     scan_inplace(s, cntB, sp.lenB, (uint32_t *)(ws + L.o_bsB), launches);
-    k_sort_b_scatter<<<(unsigned)sp.tilesB_max, SB_THREADS, sort_b_smem(sp, true), s>>>(kv, sp, seg, tb, cntB,
-                                                                                      entries);
+    e = sort_b_scatter(s, sp, kv, seg, tb, cntB, entries);
+    if (e != cudaSuccess) return e;
     *launches += 5;
   }
   k_sort_offsets<<<(unsigned)((K + 1 + 255) / 256), 256, 0, s>>>(sd, sp, K, cntA, seg, tb, cntB, offsets);
