@@ -769,6 +769,8 @@ def measure_batched(gm, wl, dev, count=512, table_log2=16):
     plan = gm.BatchPlan(table, sizes)
     out = torch.empty((count, gm.G1P_WORDS), dtype=torch.int64, device=dev)
     t_batch = time_graph(plan, sc, out)
+    out_class = torch.empty_like(out)
+    t_class = time_graph(plan.set_queue(False), sc, out_class)
     # sequential plain launches over the same slices
     rows = np.concatenate([[0], np.cumsum(sizes)])
     seq_out = torch.empty((count, gm.G1P_WORDS), dtype=torch.int64, device=dev)
@@ -786,7 +788,10 @@ def measure_batched(gm, wl, dev, count=512, table_log2=16):
            "batched_points_per_s": total / t_batch, "batched_ms": t_batch * 1e3,
            "sequential_points_per_s": total / t_seq, "sequential_ms": t_seq * 1e3,
            "speedup": t_seq / t_batch, "graph": "cuda graph replay",
-           "batched_check": check(out), "sequential_check": check(seq_out)}
+           "batched_check": check(out), "sequential_check": check(seq_out),
+           "mode": "every class's accumulation in one persistent launch over a device work queue",
+           "per_class_pipelines": {"batched_points_per_s": total / t_class, "batched_ms": t_class * 1e3,
+                                   "speedup_vs_sequential": t_seq / t_class, "check": check(out_class)}}
     plan.close()
     # the same batch over fixed-base window tables of the resident set
     t0 = time.perf_counter()
@@ -796,9 +801,13 @@ def measure_batched(gm, wl, dev, count=512, table_log2=16):
     plan = gm.BatchPlan(table, sizes)
     out_pc = torch.empty_like(out)
     t_pc = time_graph(plan, sc, out_pc)
+    out_pclass = torch.empty_like(out)
+    t_pclass = time_graph(plan.set_queue(False), sc, out_pclass)
     res["precomputed"] = {"windows": list(PRECOMPUTE_BATCH), "classes": plan.classes(),
                           "build_s": t_pre, "batched_points_per_s": total / t_pc, "batched_ms": t_pc * 1e3,
-                          "speedup_vs_sequential": t_seq / t_pc, "check": check(out_pc)}
+                          "speedup_vs_sequential": t_seq / t_pc, "check": check(out_pc),
+                          "per_class_pipelines": {"batched_points_per_s": total / t_pclass, "batched_ms": t_pclass * 1e3,
+                                                  "speedup_vs_sequential": t_seq / t_pclass, "check": check(out_pclass)}}
     plan.close()
     table.close()
     return res

@@ -63,6 +63,7 @@ C_API = [
     "gm_g1_sum_projective", "gm_g2_sum_projective", "gm_g1_msm_device_noalloc",
     "gm_bases_create", "gm_bases_destroy", "gm_bases_count", "gm_bases_precompute", "gm_msm_resident", "gm_batch_plan_create",
     "gm_batch_plan_run", "gm_batch_plan_destroy", "gm_batch_plan_bytes", "gm_batch_plan_classes",
+    "gm_batch_plan_set_queue",
     "gm_batch_run", "gm_batch_workspace_bytes", "gm_g1_sum_projective_host",
     "gm_host_selftest", "gm_fp_elem", "gm_fp2_elem", "gm_g1_point_elem", "gm_g2_point_elem",
     "gm_g1_on_curve_batch", "gm_g2_on_curve_batch", "gm_g1_msm_host_async", "gm_g2_msm_host_async",
@@ -124,6 +125,7 @@ def lib() -> ctypes.CDLL:
         L.gm_batch_plan_bytes.argtypes = [vp]
         L.gm_batch_plan_bytes.restype = i64
         L.gm_batch_plan_classes.argtypes = [vp, vp, vp, i32]
+        L.gm_batch_plan_set_queue.argtypes = [vp, i32]
         L.gm_batch_run.argtypes = [vp, vp, i32, i32, vp, vp, vp, vp, vp]
         L.gm_g1_sum_projective_host.argtypes = [vp, vp, i32]
         L.gm_batch_workspace_bytes.argtypes = [vp, i32, i32, vp, vp]
@@ -716,6 +718,14 @@ class BatchPlan:
     @property
     def workspace_bytes(self) -> int:
         return int(lib().gm_batch_plan_bytes(self.handle))
+
+    def set_queue(self, on: bool = True):
+        """Accumulation mode (gm_batch_plan_set_queue): True (the default) =
+        every class's accumulation in one persistent launch over a device work
+        queue; False = one pipeline per window class on its own stream.  Same
+        results."""
+        _check(lib().gm_batch_plan_set_queue(self.handle, 1 if on else 0), "gm_batch_plan_set_queue")
+        return self
 
     def classes(self):
         w = np.zeros(64, dtype=np.int32)

@@ -24,6 +24,8 @@ extern template int batch_run<Fp>(const BatchPlan &, cudaStream_t, const uint64_
 extern template int batch_run<Fp2>(const BatchPlan &, cudaStream_t, const uint64_t *, uint64_t *);
 extern template int window_table_launch<Fp>(cudaStream_t, const uint4 *, int64_t, int, int, uint4 *);
 extern template int window_table_launch<Fp2>(cudaStream_t, const uint4 *, int64_t, int, int, uint4 *);
+extern template int batch_queue_setup<Fp>(BatchPlan &);
+extern template int batch_queue_setup<Fp2>(BatchPlan &);
 }  // namespace gm
 
 struct gm_bases {
@@ -58,8 +60,12 @@ void free_plan(gm_batch_plan *p) {
     if (cp.desc) cudaFree(cp.desc);
     if (cp.stream) cudaStreamDestroy(cp.stream);
     if (cp.done) cudaEventDestroy(cp.done);
+    if (cp.sorted) cudaEventDestroy(cp.sorted);
   }
   if (p->plan.fork) cudaEventDestroy(p->plan.fork);
+  if (p->plan.acc_done) cudaEventDestroy(p->plan.acc_done);
+  if (p->plan.acc_desc) cudaFree(p->plan.acc_desc);
+  if (p->plan.queue_ctr) cudaFree(p->plan.queue_ctr);
   delete p;
 }
 
@@ -297,6 +303,7 @@ int gm_batch_plan_create(const gm_bases *b, int scalar_limbs, int count, const i
     if (e == cudaSuccess) e = cudaMalloc(&cp.ws, cp.ws_bytes);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&cp.stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&cp.done, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&cp.sorted, cudaEventDisableTiming);
     if (e != cudaSuccess) {
       free_plan(p);
       gm::record_error(e, "batch plan allocation");
@@ -305,11 +312,29 @@ int gm_batch_plan_create(const gm_bases *b, int scalar_limbs, int count, const i
     plan.bytes += cp.ws_bytes + desc_bytes;
   }
   cudaError_t e = cudaEventCreateWithFlags(&plan.fork, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&plan.acc_done, cudaEventDisableTiming);
+  // descriptors of the queued accumulation (used when the plan's mode is set)
+  const size_t desc_bytes = plan.classes.size() *
+                            (plan.group == 1 ? sizeof(gm::AccClass<gm::Fp>) : sizeof(gm::AccClass<gm::Fp2>));
+  if (e == cudaSuccess) e = cudaMalloc(&plan.acc_desc, desc_bytes);
+  if (e == cudaSuccess) e = cudaMalloc(&plan.queue_ctr, sizeof(uint32_t));
   if (e != cudaSuccess) {
     free_plan(p);
-    return gm::record_error(e, "cudaEventCreate");
+    return gm::record_error(e, "batch plan events / queue");
   }
+  rc = plan.group == 1 ? gm::batch_queue_setup<gm::Fp>(plan) : gm::batch_queue_setup<gm::Fp2>(plan);
+  if (rc) {
+    free_plan(p);
+    return rc;
+  }
+  plan.bytes += desc_bytes + sizeof(uint32_t);
   *out = p;
+  return gm::GM_OK;
+}
+
+int gm_batch_plan_set_queue(gm_batch_plan *p, int on) {
+  if (!p) return gm::GM_ERR_ARG;
+  p->plan.queue = on != 0;
   return gm::GM_OK;
 }
 

@@ -9,5 +9,6 @@ template int msm_run<Fp>(cudaStream_t, const MsmLayout<Fp> &, char *, const uint
                          const uint64_t *, uint64_t *, bool, uint32_t *, cudaEvent_t);
 template int batch_layouts<Fp>(BatchPlan &, int);
 template int batch_run<Fp>(const BatchPlan &, cudaStream_t, const uint64_t *, uint64_t *);
+template int batch_queue_setup<Fp>(BatchPlan &);
 template int window_table_launch<Fp>(cudaStream_t, const uint4 *, int64_t, int, int, uint4 *);
 }  // namespace gm

@@ -103,27 +103,26 @@ struct AccOccupancy {
   size_t smem = 0;    // dynamic shared memory of a launch
 };
 
+// which: 0 = k_accumulate<F>, 1 = k_accumulate_queue<F> (same limits)
 template <class F>
-static AccOccupancy acc_occupancy(int dev) {
+static AccOccupancy acc_occupancy(int dev, int which = 0) {
   static std::mutex mu;
-  static AccOccupancy cached[64];
+  static AccOccupancy cached[2][64];
   std::lock_guard<std::mutex> lk(mu);
   if (dev < 0 || dev >= 64) dev = 0;
-  AccOccupancy &o = cached[dev];
+  AccOccupancy &o = cached[which][dev];
+  const void *fn = which == 0 ? (const void *)k_accumulate<F> : (const void *)k_accumulate_queue<F>;
   if (o.blocks == 0) {
     size_t smem = acc_smem_bytes<F>();
     int per_sm_smem = 0, b = 0;
     cudaDeviceGetAttribute(&per_sm_smem, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
-    cudaFuncSetAttribute(k_accumulate<F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_accumulate<F>, ACC_THREADS, smem) != cudaSuccess) b = 1;
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, ACC_THREADS, smem) != cudaSuccess) b = 1;
     if (b > ACC_BLOCKS_MAX && per_sm_smem > 0) {
       // (ACC_BLOCKS_MAX + 1) blocks must not fit in the SM's shared memory
       const size_t pad = (size_t)per_sm_smem / (ACC_BLOCKS_MAX + 1) + 1024;
-      if (cudaFuncSetAttribute(k_accumulate<F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pad) ==
-          cudaSuccess)
-        smem = pad;
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_accumulate<F>, ACC_THREADS, smem) != cudaSuccess)
-        b = 1;
+      if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pad) == cudaSuccess) smem = pad;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, ACC_THREADS, smem) != cudaSuccess) b = 1;
     }
     o.smem = smem;
     o.blocks = std::max(1, std::min(b, ACC_BLOCKS_MAX));

@@ -412,20 +412,15 @@ struct StagedPoint {
 // laid out chunk-major ([slot][chunk][thread]) so a warp's 16-byte accesses
 // hit consecutive banks.  Only the owning thread reads its slots, so no
 // block-level barrier is needed.
-template <class F>
-__global__ void __launch_bounds__(ACC_THREADS) k_accumulate(const uint4 *__restrict__ bases, const uint32_t *__restrict__ entries,
-                                                    const uint32_t *__restrict__ offsets, int64_t K, int64_t nthreads,
-                                                    xyzz_t<F> *__restrict__ buckets,
-                                                    xyzz_t<F> *__restrict__ part_head, xyzz_t<F> *__restrict__ part_tail,
-                                                    int32_t *__restrict__ head_key, int32_t *__restrict__ tail_key) {
-  using T = typename F::T;
+// One accumulation slice t of nthreads equal slices of the sorted entries
+// (its stage: this thread's two shared-memory slots).
+template <class F, int CH>
+GM_DEVI void acc_slice(const uint4 *__restrict__ bases, const uint32_t *__restrict__ entries,
+                       const uint32_t *__restrict__ offsets, int64_t K, int64_t nthreads, int64_t t,
+                       xyzz_t<F> *__restrict__ buckets, xyzz_t<F> *__restrict__ part_head,
+                       xyzz_t<F> *__restrict__ part_tail, int32_t *__restrict__ head_key,
+                       int32_t *__restrict__ tail_key, uint4 (*stage)[CH][ACC_THREADS], int tid) {
   using FA = typename AccPolicy<F>::type;
-  constexpr int CH = F::LIMBS / 2;  // 16-byte chunks of x || y
-  extern __shared__ uint4 stage_mem[];  // [2][CH][ACC_THREADS], acc_smem_bytes<F>()
-  auto stage = reinterpret_cast<uint4(*)[CH][ACC_THREADS]>(stage_mem);
-  const int tid = threadIdx.x;
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= nthreads) return;
   int32_t hk = -1, tk = -1;
   // slice length from the actual number of entries (offsets[K])
   const uint32_t M = __ldg(offsets + K);
@@ -489,6 +484,74 @@ __global__ void __launch_bounds__(ACC_THREADS) k_accumulate(const uint4 *__restr
   }
   head_key[t] = hk;
   tail_key[t] = tk;
+}
+
+// The base of the next entry is staged into shared memory with cp.async while
+// the current mixed addition runs, so the random 112/224-byte gather is off
+// the critical path.  Each thread owns two slots (double buffer); slots are
+// laid out chunk-major ([slot][chunk][thread]) so a warp's 16-byte accesses
+// hit consecutive banks.  Only the owning thread reads its slots, so no
+// block-level barrier is needed.
+template <class F>
+__global__ void __launch_bounds__(ACC_THREADS) k_accumulate(const uint4 *__restrict__ bases, const uint32_t *__restrict__ entries,
+                                                    const uint32_t *__restrict__ offsets, int64_t K, int64_t nthreads,
+                                                    xyzz_t<F> *__restrict__ buckets,
+                                                    xyzz_t<F> *__restrict__ part_head, xyzz_t<F> *__restrict__ part_tail,
+                                                    int32_t *__restrict__ head_key, int32_t *__restrict__ tail_key) {
+  constexpr int CH = F::LIMBS / 2;  // 16-byte chunks of x || y
+  extern __shared__ uint4 stage_mem[];  // [2][CH][ACC_THREADS], acc_smem_bytes<F>()
+  auto stage = reinterpret_cast<uint4(*)[CH][ACC_THREADS]>(stage_mem);
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nthreads) return;
+  acc_slice<F, CH>(bases, entries, offsets, K, nthreads, t, buckets, part_head, part_tail, head_key, tail_key, stage,
+                   threadIdx.x);
+}
+
+// One class of a batch in the queued accumulation: its slicing (nthreads
+// equal slices, a multiple of 32) and buffers, and its first work item.
+template <class F>
+struct AccClass {
+  const uint4 *bases;
+  const uint32_t *entries, *offsets;
+  int64_t K, nthreads;
+  xyzz_t<F> *buckets, *head, *tail;
+  int32_t *hk, *tk;
+  int64_t item_first;
+};
+
+// Accumulation of every class of a batch in one persistent launch (one
+// resident wave) over a device work queue: a work item is 32 consecutive
+// slices of one class, taken by a warp from the counter *queue (zero on
+// entry); the slicing and outputs are those of k_accumulate, class by class,
+// so the fix-up and reduction of each class follow unchanged.
+template <class F>
+__global__ void __launch_bounds__(ACC_THREADS) k_accumulate_queue(const AccClass<F> *__restrict__ cls, int ncls,
+                                                                  int64_t items, uint32_t *__restrict__ queue) {
+  constexpr int CH = F::LIMBS / 2;
+  extern __shared__ uint4 stage_mem[];
+  auto stage = reinterpret_cast<uint4(*)[CH][ACC_THREADS]>(stage_mem);
+  const int lane = threadIdx.x & 31;
+  while (true) {
+    uint32_t item = 0;
+    if (lane == 0) item = atomicAdd(queue, 1u);
+    item = __shfl_sync(0xffffffffu, item, 0);
+    if ((int64_t)item >= items) break;
+    int lo = 0, hi = ncls;  // cls[lo].item_first <= item < cls[hi].item_first
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (cls[mid].item_first <= (int64_t)item)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    const AccClass<F> c = cls[lo];
+    const int64_t t = ((int64_t)item - c.item_first) * 32 + lane;
+    acc_slice<F, CH>(c.bases, c.entries, c.offsets, c.K, c.nthreads, t, c.buckets, c.head, c.tail, c.hk, c.tk, stage,
+                     threadIdx.x);
+    // the next item reuses this thread's stage slots
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    __syncwarp();
+  }
 }
 
 }  // namespace gm

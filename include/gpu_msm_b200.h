@@ -204,6 +204,13 @@ int gm_msm_resident(gm_stream_t stream, const gm_bases *bases, int64_t base_offs
 int gm_batch_plan_create(const gm_bases *bases, int scalar_limbs, int count, const int64_t *sizes,
                          const int64_t *base_offsets, const int32_t *window_bits, gm_batch_plan **out);
 int gm_batch_plan_run(gm_batch_plan *plan, gm_stream_t stream, const uint64_t *d_scalars, void *d_results);
+/* Accumulation mode of a plan (no reference counterpart): 1 (default) = the
+ * accumulation of every window class in one persistent launch over a device
+ * work queue of (class, 32 slices) items, between the classes' sorts and
+ * their fix-ups; 0 = one pipeline per window class, each on its own stream
+ * with full-GPU kernels.  Results are identical; the mode only changes
+ * scheduling. */
+int gm_batch_plan_set_queue(gm_batch_plan *p, int on);
 int gm_batch_plan_destroy(gm_batch_plan *plan);
 int64_t gm_batch_plan_bytes(const gm_batch_plan *plan);
 int gm_batch_plan_classes(const gm_batch_plan *plan, int32_t *window_bits, int32_t *counts, int max);

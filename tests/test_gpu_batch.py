@@ -84,7 +84,13 @@ def test_batch_mixed_window_classes(cuda):
     assert sorted(w for w, _ in plan.classes()) == [3, 7, 11]
     res = plan.run(t_dev(sc, cuda).reshape(-1, 5))
     torch.cuda.synchronize()
-    check(res, expected(sizes, offs, sc, logs, 1), 1)
+    want = expected(sizes, offs, sc, logs, 1)
+    check(res, want, 1)
+    plan.set_queue(False)
+    res_q = plan.run(t_dev(sc, cuda).reshape(-1, 5))
+    torch.cuda.synchronize()
+    check(res_q, want, 1)
+    assert torch.equal(res_q, res)
 
 
 def test_batch_graph_capture_replay(cuda):
@@ -260,18 +266,37 @@ def test_batch_512_config_every_output(cuda):
         torch.cuda.synchronize()
         _check_all(out, sizes, sc, logs)
     del g
-    plan.close()
-    for c in (8, 10, 12, 14, 16):
-        table.precompute(c)
-    plan = gm.BatchPlan(table, sizes)
+    # the same plan with one pipeline per class (the other accumulation mode)
+    plan.set_queue(False)
+    first = None
     g = graph_of(plan)
-    for seed in (7373, 7474):
+    for seed in (7575, 7575):
         sc = wl.make_scalars(total, seed=seed)
         static_sc.copy_(t_dev(sc, cuda).reshape(-1, 5))
         out.zero_()
         g.replay()
         torch.cuda.synchronize()
         _check_all(out, sizes, sc, logs)
+        # deterministic whatever order the queue hands out the work
+        if first is None:
+            first = out.clone()
+        else:
+            assert torch.equal(out, first)
     del g
+    plan.close()
+    for c in (8, 10, 12, 14, 16):
+        table.precompute(c)
+    plan = gm.BatchPlan(table, sizes)
+    for queue in (True, False):
+        plan.set_queue(queue)
+        g = graph_of(plan)
+        for seed in (7373, 7474):
+            sc = wl.make_scalars(total, seed=seed)
+            static_sc.copy_(t_dev(sc, cuda).reshape(-1, 5))
+            out.zero_()
+            g.replay()
+            torch.cuda.synchronize()
+            _check_all(out, sizes, sc, logs)
+        del g
     plan.close()
     table.close()
