@@ -63,7 +63,7 @@ C_API = [
     "gm_g1_sum_projective", "gm_g2_sum_projective", "gm_g1_msm_device_noalloc",
     "gm_bases_create", "gm_bases_destroy", "gm_bases_count", "gm_bases_precompute", "gm_msm_resident", "gm_batch_plan_create",
     "gm_batch_plan_run", "gm_batch_plan_destroy", "gm_batch_plan_bytes", "gm_batch_plan_classes",
-    "gm_batch_plan_set_queue",
+    "gm_batch_plan_set_queue", "gm_batch_plan_create_tuned",
     "gm_batch_run", "gm_batch_workspace_bytes", "gm_g1_sum_projective_host",
     "gm_host_selftest", "gm_fp_elem", "gm_fp2_elem", "gm_g1_point_elem", "gm_g2_point_elem",
     "gm_g1_on_curve_batch", "gm_g2_on_curve_batch", "gm_g1_msm_host_async", "gm_g2_msm_host_async",
@@ -126,6 +126,7 @@ def lib() -> ctypes.CDLL:
         L.gm_batch_plan_bytes.restype = i64
         L.gm_batch_plan_classes.argtypes = [vp, vp, vp, i32]
         L.gm_batch_plan_set_queue.argtypes = [vp, i32]
+        L.gm_batch_plan_create_tuned.argtypes = [vp, i32, i32, vp, vp, vp, vp, vp]
         L.gm_batch_run.argtypes = [vp, vp, i32, i32, vp, vp, vp, vp, vp]
         L.gm_g1_sum_projective_host.argtypes = [vp, vp, i32]
         L.gm_batch_workspace_bytes.argtypes = [vp, i32, i32, vp, vp]
@@ -680,14 +681,25 @@ def window_table() -> dict:
     return _WINDOW_TABLE
 
 
+def tuned_params(group: int, n: int, scalar_limbs: int = 5):
+    """(window width, accumulation slice waves, sort points per thread) for an
+    MSM of n points: the autotuned values of its size class floor(log2 n)
+    when tuned, else (cost model, 1, 4).  Table entries are either a width
+    or {"c": .., "slice_waves": .., "sort_ppt": ..}."""
+    tab = window_table().get(f"g{group}", {})
+    e = max(0, int(n).bit_length() - 1)
+    v = tab.get(str(e))
+    if isinstance(v, dict):
+        return int(v["c"]), int(v.get("slice_waves", 1)), int(v.get("sort_ppt", 4))
+    if v is not None:
+        return int(v), 1, 4
+    return default_window(group, n, scalar_limbs), 1, 4
+
+
 def tuned_window(group: int, n: int, scalar_limbs: int = 5) -> int:
     """Window width for an MSM of n points: the autotuned value for its size
     class floor(log2 n) when tuned, else the library's cost model."""
-    tab = window_table().get(f"g{group}", {})
-    e = max(0, int(n).bit_length() - 1)
-    if str(e) in tab:
-        return int(tab[str(e)])
-    return default_window(group, n, scalar_limbs)
+    return tuned_params(group, n, scalar_limbs)[0]
 
 
 class BatchPlan:
@@ -698,7 +710,10 @@ class BatchPlan:
     current (or given) stream; it only launches kernels, so it can be captured
     in a CUDA graph and replayed with new scalars in the same tensor."""
 
-    def __init__(self, bases: ResidentBases, sizes, base_offsets=None, window_bits=None, scalar_limbs: int = 5):
+    def __init__(self, bases: ResidentBases, sizes, base_offsets=None, window_bits=None, scalar_limbs: int = 5,
+                 tuning=None):
+        """tuning: None = the autotuned (slice waves, sort points per thread)
+        of each MSM's size class; or an int32 array (count, 2)."""
         self.bases = bases
         self.sizes = np.ascontiguousarray(sizes, dtype=np.int64)
         self.count = len(self.sizes)
@@ -708,12 +723,15 @@ class BatchPlan:
         if window_bits is None:
             window_bits = bases.windows_for(self.sizes, scalar_limbs)
         wins = np.ascontiguousarray(window_bits, dtype=np.int32)
+        if tuning is None:
+            tuning = [tuned_params(bases.group, int(n), scalar_limbs)[1:] for n in self.sizes]
+        tun = np.ascontiguousarray(np.asarray(tuning, dtype=np.int32).reshape(self.count, 2))
         h = ctypes.c_void_p()
-        _check(lib().gm_batch_plan_create(bases.handle, scalar_limbs, self.count, _p(self.sizes),
-                                          None if offs is None else _p(offs), None if wins is None else _p(wins),
-                                          ctypes.byref(h)), "gm_batch_plan_create")
+        _check(lib().gm_batch_plan_create_tuned(bases.handle, scalar_limbs, self.count, _p(self.sizes),
+                                                None if offs is None else _p(offs), _p(wins), _p(tun),
+                                                ctypes.byref(h)), "gm_batch_plan_create_tuned")
         self.handle = h
-        self._keep = (offs, wins)
+        self._keep = (offs, wins, tun)
 
     @property
     def workspace_bytes(self) -> int:

@@ -1,14 +1,22 @@
-"""Window-width autotuner.
+"""Batch-plan autotuner.
 
 For each group and size class e = floor(log2 n), builds a batch of MSMs of
-2^e points over a resident synthetic table, times the batched pipeline for
-each candidate window width c (CUDA events, after a warm-up run) and records
-the fastest in ``window_table.json`` next to this file:
+2^e points over a resident synthetic table and times the batched pipeline
+(CUDA events, after a warm-up run) for
+  1. each candidate window width c around the cost model (defaults for the rest);
+  2. at the best c, the accumulation slices of the class in resident waves of
+     threads (1, 2, 4: finer work items for the queued accumulation, more
+     partials for the fix-up);
+  3. at those, the pass-A sort tile in points per thread (2, 4, 8: 512, 1024
+     or 2048 points per tile: fewer, larger tiles mean fewer counters to scan,
+     smaller ones more blocks)
+and records the fastest in ``window_table.json`` next to this file:
 
-    {"g1": {"8": 7, ...}, "g2": {...}, "device": "...", "points_per_class": N}
+    {"g1": {"8": {"c": 7, "slice_waves": 1, "sort_ppt": 4}, ...}, "g2": {...},
+     "device": "...", "points_per_class": N}
 
-``gpu_msm_b200.tuned_window(group, n)`` reads it; batch plans use it for
-every MSM whose window width is not given.  Run on the target GPU:
+``gpu_msm_b200.tuned_params(group, n)`` reads it; batch plans use it for every
+MSM whose parameters are not given.  Run on the target GPU:
 
     python -m gpu_msm_b200.autotune [--quick]
 """
@@ -58,18 +66,29 @@ def tune_group(group, lo, hi, points_per_class, reps, dev):
         rng = np.random.default_rng(e)
         offs = rng.integers(0, n_table - n + 1, size=count).astype(np.int64)
         sc = torch.from_numpy(wl.make_scalars(count * n, seed=1000 + e).view(np.int64)).to(dev)
+
+        def run(c, waves, ppt):
+            plan = gm.BatchPlan(table, sizes, offs, window_bits=np.full(count, c, dtype=np.int32),
+                                tuning=np.tile(np.array([waves, ppt], dtype=np.int32), (count, 1)))
+            t = _time_plan(plan, sc, reps)
+            plan.close()
+            return t
+
         model = gm.default_window(group, n, 5)
         cands = sorted(set(c for c in range(max(2, model - 3), min(20, model + 2) + 1)))
-        times = {}
-        for c in cands:
-            plan = gm.BatchPlan(table, sizes, offs, window_bits=np.full(count, c, dtype=np.int32))
-            times[c] = _time_plan(plan, sc, reps)
-            plan.close()
-        best = min(times, key=times.get)
-        result[str(e)] = int(best)
-        detail[str(e)] = {"count": count, "ms": {str(c): round(t, 3) for c, t in times.items()}, "model": model}
-        print(f"g{group} 2^{e:2d} x{count:4d}: best c={best:2d} ({times[best]:.3f} ms), cost model {model}",
-              flush=True)
+        t_c = {c: run(c, 1, 4) for c in cands}
+        c = min(t_c, key=t_c.get)
+        t_w = {w: (t_c[c] if w == 1 else run(c, w, 4)) for w in (1, 2, 4)}
+        waves = min(t_w, key=t_w.get)
+        t_p = {q: (t_w[waves] if q == 4 else run(c, waves, q)) for q in (2, 4, 8)}
+        ppt = min(t_p, key=t_p.get)
+        result[str(e)] = {"c": int(c), "slice_waves": int(waves), "sort_ppt": int(ppt)}
+        detail[str(e)] = {"count": count, "model": model,
+                          "ms_by_c": {str(k): round(v, 3) for k, v in t_c.items()},
+                          "ms_by_slice_waves": {str(k): round(v, 3) for k, v in t_w.items()},
+                          "ms_by_sort_ppt": {str(k): round(v, 3) for k, v in t_p.items()}}
+        print(f"g{group} 2^{e:2d} x{count:4d}: c={c:2d} waves={waves} ppt={ppt} ({t_p[ppt]:.3f} ms; "
+              f"c alone {t_c[c]:.3f} ms), cost model {model}", flush=True)
     table.close()
     return result, detail
 

@@ -72,9 +72,13 @@ void free_plan(gm_batch_plan *p) {
 // Validates the batch, groups MSMs by window width and computes each class's
 // layout; d64[k] / idx[k] receive class k's descriptors
 // (point_start | base_off | sc_off, and out_index | tile_first).
+// tuning (optional): per MSM, the accumulation slices of its class in
+// resident waves (tuning[2 i]: 1, 2 or 4; 0 = 1) and the pass-A sort tile in
+// points per thread (tuning[2 i + 1]: 2, 4 or 8; 0 = 4); a class takes the
+// values of its largest MSM.
 int build_classes(const gm_bases *b, int scalar_limbs, int count, const int64_t *sizes, const int64_t *base_offsets,
                   const int32_t *window_bits, gm::BatchPlan &plan, std::vector<std::vector<int64_t>> &d64,
-                  std::vector<std::vector<int32_t>> &idx) {
+                  std::vector<std::vector<int32_t>> &idx, const int32_t *tuning = nullptr) {
   if (!b || count <= 0 || !sizes || scalar_limbs < 1 || scalar_limbs > gm::MAX_SCALAR_LIMBS) return gm::GM_ERR_ARG;
   int rc = gm::select_device((uint32_t)b->dev);
   if (rc) return rc;
@@ -120,9 +124,26 @@ int build_classes(const gm_bases *b, int scalar_limbs, int count, const int64_t 
     gm::BatchClassPlan cp;
     cp.c = kv.first;
     cp.count = (int)kv.second.size();
+    int largest = kv.second[0];
+    for (int i : kv.second)
+      if (sizes[i] > sizes[largest]) largest = i;
+    if (tuning) {
+      const int waves = tuning[2 * largest], ppt = tuning[2 * largest + 1];
+      if (waves != 0 && waves != 1 && waves != 2 && waves != 4) {
+        gm::set_last_error("batch tuning: slice waves must be 1, 2 or 4");
+        return gm::GM_ERR_ARG;
+      }
+      if (ppt != 0 && ppt != 2 && ppt != 4 && ppt != 8) {
+        gm::set_last_error("batch tuning: sort tile must be 2, 4 or 8 points per thread");
+        return gm::GM_ERR_ARG;
+      }
+      cp.slice_waves = waves ? waves : 1;
+      cp.sort_ppt = ppt ? ppt : gm::SA_PPT;
+    }
+    const int64_t tp = (int64_t)gm::SA_THREADS * cp.sort_ppt;
     for (int i : kv.second) {
       cp.P += sizes[i];
-      cp.tilesA += (sizes[i] + gm::SA_TP - 1) / gm::SA_TP;
+      cp.tilesA += (sizes[i] + tp - 1) / tp;
     }
     if (const auto *t = b->table_for(cp.c, gm::windows_for(cp.c, scalar_limbs))) {
       cp.pc_table = t->table;
@@ -164,7 +185,8 @@ int build_classes(const gm_bases *b, int scalar_limbs, int count, const int64_t 
       v[2 * cp.count + 1 + j] = sc_row[i];
       idx[k][j] = i;
       idx[k][cp.count + j] = tiles;
-      tiles += (int32_t)((sizes[i] + gm::SA_TP - 1) / gm::SA_TP);
+      const int64_t tp = (int64_t)gm::SA_THREADS * cp.sort_ppt;
+      tiles += (int32_t)((sizes[i] + tp - 1) / tp);
     }
     v[cp.count] = acc;
     idx[k][2 * (size_t)cp.count] = tiles;
@@ -281,12 +303,18 @@ int gm_msm_resident(gm_stream_t stream, const gm_bases *b, int64_t base_offset, 
 
 int gm_batch_plan_create(const gm_bases *b, int scalar_limbs, int count, const int64_t *sizes,
                          const int64_t *base_offsets, const int32_t *window_bits, gm_batch_plan **out) {
+  return gm_batch_plan_create_tuned(b, scalar_limbs, count, sizes, base_offsets, window_bits, nullptr, out);
+}
+
+int gm_batch_plan_create_tuned(const gm_bases *b, int scalar_limbs, int count, const int64_t *sizes,
+                               const int64_t *base_offsets, const int32_t *window_bits, const int32_t *tuning,
+                               gm_batch_plan **out) {
   if (!b || !out) return gm::GM_ERR_ARG;
   auto *p = new (std::nothrow) gm_batch_plan;
   if (!p) return gm::GM_ERR_ALLOC;
   std::vector<std::vector<int64_t>> d64;
   std::vector<std::vector<int32_t>> idx;
-  int rc = build_classes(b, scalar_limbs, count, sizes, base_offsets, window_bits, p->plan, d64, idx);
+  int rc = build_classes(b, scalar_limbs, count, sizes, base_offsets, window_bits, p->plan, d64, idx, tuning);
   if (rc) {
     delete p;
     return rc;

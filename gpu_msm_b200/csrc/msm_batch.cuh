@@ -22,7 +22,9 @@ struct BatchClassPlan {
   int count = 0;        // MSMs in this class
   int64_t P = 0;        // points in this class
   int64_t K = 0, nthreads = 0;
-  int64_t tilesA = 0;   // pass-A sort tiles (SA_TP points, one MSM each)
+  int64_t tilesA = 0;   // pass-A sort tiles (SA_THREADS * sort_ppt points, one MSM each)
+  int slice_waves = 1;  // accumulation slices: this many resident waves of threads
+  int sort_ppt = SA_PPT;  // pass-A sort tile: points per thread (2, 4 or 8)
   SortLayout sl;
   RedLayout rl;
   int64_t long_cap = 0;
@@ -74,13 +76,13 @@ void batch_class_layout(BatchClassPlan &cp, int limbs, int sms, int dev) {
   // precomputed mode: one bucket set per MSM (no window index in the key)
   const int64_t groups = (int64_t)cp.count * (cp.pc_stride ? 1 : cp.dp.W);
   cp.K = groups * cp.dp.B;
-  cp.nthreads = (int64_t)sms * acc_blocks_per_sm<F>(dev) * ACC_THREADS;
+  cp.nthreads = (int64_t)sms * acc_blocks_per_sm<F>(dev) * ACC_THREADS * cp.slice_waves;
   const int64_t max_entries = cp.P * cp.dp.W;
   if (cp.nthreads > max_entries) cp.nthreads = std::max<int64_t>(1, (max_entries + 127) / 128 * 128);
   Carve cv;
   cp.o_offsets = cv.take<uint32_t>(cp.K + 1);
   cp.o_entries = cv.take<uint32_t>((size_t)std::max<int64_t>(1, max_entries));
-  cp.sl.plan(cp.dp, cp.count, cp.P, cp.tilesA, cp.pc_stride != 0, cv);
+  cp.sl.plan(cp.dp, cp.count, cp.P, cp.tilesA, cp.pc_stride != 0, cv, cp.sort_ppt);
   cp.o_buckets = cv.take<xyzz_t<F>>(cp.K);
   cp.o_head = cv.take<xyzz_t<F>>(cp.nthreads);
   cp.o_tail = cv.take<xyzz_t<F>>(cp.nthreads);

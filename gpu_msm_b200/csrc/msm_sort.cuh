@@ -9,7 +9,8 @@
 // reference has no sort: its kernels scan all n points for every bucket
 // (src/curve.cu:1180-1371, :1659-1728).
 //
-// Pass A reads the scalars once per tile of SA_TP points (one MSM per tile),
+// Pass A reads the scalars once per tile of SA_THREADS * ppt points (one MSM
+// per tile; ppt = 2, 4 or 8 points per thread, chosen per plan),
 // staged in shared memory, computes the digits window by window, and
 // partitions the entries by (group, hi) where hi = b >> LB: every block
 // counts its tile's entries per (group, hi) with shared-memory atomics
@@ -40,8 +41,8 @@
 namespace gm {
 
 constexpr int SA_THREADS = 256;
-constexpr int SA_PPT = 4;                        // points per thread (pass A)
-constexpr int SA_TP = SA_THREADS * SA_PPT;       // points per pass-A tile
+constexpr int SA_PPT = 4;                        // default points per thread (pass A): 2, 4 or 8
+constexpr int SA_TP = SA_THREADS * SA_PPT;       // default points per pass-A tile
 constexpr int SB_THREADS = 256;
 constexpr int SB_IPT = 8;                        // entries per thread (pass B)
 constexpr int SB_TILE = SB_THREADS * SB_IPT;     // entries per pass-B tile
@@ -69,6 +70,8 @@ struct SortParams {
   int64_t lenB = 0;    // pass-B counters (upper bound)
   int64_t tilesA = 0;
   int64_t tilesB_max = 0;
+  int ppt = SA_PPT;          // pass-A points per thread (2, 4 or 8)
+  int tp = SA_TP;            // pass-A points per tile (SA_THREADS * ppt)
 };
 
 struct TileA {
@@ -82,8 +85,8 @@ GM_DEVI TileA tile_a_info(const SortDesc &sd, const SortParams &sp, int tile) {
     ti.i = 0;
     ti.t = tile;
     ti.tiles = (int)sp.tilesA;
-    ti.p0 = (int64_t)tile * SA_TP;
-    ti.np = min((int64_t)SA_TP, sd.n_single - ti.p0);
+    ti.p0 = (int64_t)tile * sp.tp;
+    ti.np = min((int64_t)sp.tp, sd.n_single - ti.p0);
     ti.base_off = ti.p0;
     ti.sc_row = ti.p0;
     ti.cbase = 0;
@@ -102,9 +105,9 @@ GM_DEVI TileA tile_a_info(const SortDesc &sd, const SortParams &sp, int tile) {
   ti.t = tile - f0;
   ti.tiles = __ldg(sd.tile_first + lo + 1) - f0;
   const int64_t ps = __ldg(sd.point_start + lo), pe = __ldg(sd.point_start + lo + 1);
-  const int64_t j0 = (int64_t)ti.t * SA_TP;
+  const int64_t j0 = (int64_t)ti.t * sp.tp;
   ti.p0 = ps + j0;
-  ti.np = min((int64_t)SA_TP, pe - ti.p0);
+  ti.np = min((int64_t)sp.tp, pe - ti.p0);
   ti.base_off = __ldg(sd.base_off + lo) + j0;
   ti.sc_row = __ldg(sd.sc_off + lo) + j0;
   ti.cbase = (int64_t)sp.S * sp.RA * f0;
@@ -169,27 +172,27 @@ __host__ __device__ inline int sort_a_blocks_per_tile(const SortParams &sp) {
 // the counters [S][RA]; for the scatter, the per-warp counters
 // [SORT_WARPS][groups][RA] and a running count per hi.
 inline size_t sort_a_smem(const SortParams &sp, bool scatter) {
-  if (!scatter) return (size_t)SA_TP * sp.dp.limbs * sizeof(uint64_t) + (size_t)sp.S * sp.RA * sizeof(uint32_t);
+  if (!scatter) return (size_t)sp.tp * sp.dp.limbs * sizeof(uint64_t) + (size_t)sp.S * sp.RA * sizeof(uint32_t);
   const size_t GR = (size_t)sort_a_groups(sp) * sp.RA;
   return (SORT_WARPS * GR + sp.RA) * sizeof(uint32_t);
 }
 
 // Signed digits of the pass-A tiles, written by the counting kernel and read
-// by the scatter: dig[(tile * W + w) * SA_TP + q] for point slot q.
-GM_DEVI int64_t dig_index(int tile, int W, int w, int q) { return ((int64_t)tile * W + w) * SA_TP + q; }
+// by the scatter: dig[(tile * W + w) * tp + q] for point slot q.
+GM_DEVI int64_t dig_index(int tile, int W, int w, int q, int tp) { return ((int64_t)tile * W + w) * tp + q; }
 
 // Digits of the tile's points for windows [w0, w1), in (warp, round, lane)
-// order: warp wp takes points [32 SA_PPT wp, 32 SA_PPT (wp + 1)), 32 per
+// order: warp wp takes points [32 PPT wp, 32 PPT (wp + 1)), 32 per
 // round; carry[] holds each point's carry into window w0 and is advanced.
 // fn(w, q, d) for every window and point slot (d = 0: no entry).
-template <class Fn>
+template <int PPT, class Fn>
 GM_DEVI void tile_digits(const uint64_t *sc, const TileA &ti, const SortParams &sp, int w0, int w1,
-                         uint32_t (&carry)[SA_PPT], Fn fn) {
+                         uint32_t (&carry)[PPT], Fn fn) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, limbs = sp.dp.limbs;
   for (int w = w0; w < w1; w++) {
 #pragma unroll
-    for (int r = 0; r < SA_PPT; r++) {
-      const int q = warp * (32 * SA_PPT) + r * 32 + lane;
+    for (int r = 0; r < PPT; r++) {
+      const int q = warp * (32 * PPT) + r * 32 + lane;
       int d = 0;
       if (q < ti.np) d = signed_digit(sc + (size_t)q * limbs, limbs, w, sp.dp, carry[r]);
       fn(w, q, d);
@@ -208,21 +211,22 @@ GM_DEVI void stage_scalars(uint64_t *sc, const uint64_t *scalars, const TileA &t
 // Pass A, counting: the tile's signed digits (into dig) and its entries per
 // (group in MSM, hi digit), counted with shared-memory atomics; writes every
 // counter of the tile.
-static __global__ void __launch_bounds__(SA_THREADS) k_sort_a_count(const uint64_t *__restrict__ scalars, SortDesc sd,
+template <int PPT>
+__global__ void __launch_bounds__(SA_THREADS) k_sort_a_count(const uint64_t *__restrict__ scalars, SortDesc sd,
                                                                   SortParams sp, uint32_t *__restrict__ cnt,
                                                                   int32_t *__restrict__ dig) {
   extern __shared__ uint64_t sort_smem[];
   const int limbs = sp.dp.limbs, RA = sp.RA, SR = sp.S * RA, W = sp.dp.W;
   uint64_t *sc = sort_smem;
-  uint32_t *h = reinterpret_cast<uint32_t *>(sc + (size_t)SA_TP * limbs);  // [S][RA]
+  uint32_t *h = reinterpret_cast<uint32_t *>(sc + (size_t)sp.tp * limbs);  // [S][RA]
   const TileA ti = tile_a_info(sd, sp, blockIdx.x);
   stage_scalars(sc, scalars, ti, limbs);
   for (int k = threadIdx.x; k < SR; k += SA_THREADS) h[k] = 0;
   __syncthreads();
   const int shift = sp.passes == 2 ? sp.LB : 0;
-  uint32_t carry[SA_PPT] = {0};
-  tile_digits(sc, ti, sp, 0, W, carry, [&](int w, int q, int d) {
-    dig[dig_index(blockIdx.x, W, w, q)] = d;
+  uint32_t carry[PPT] = {0};
+  tile_digits<PPT>(sc, ti, sp, 0, W, carry, [&](int w, int q, int d) {
+    dig[dig_index(blockIdx.x, W, w, q, sp.tp)] = d;
     if (d == 0) return;
     const uint32_t b = (uint32_t)(d < 0 ? -d : d) - 1u;
     atomicAdd(&h[(sp.S == 1 ? 0 : w) * RA + (b >> shift)], 1u);
@@ -237,8 +241,9 @@ static __global__ void __launch_bounds__(SA_THREADS) k_sort_a_count(const uint64
 // of the tile's output range (and, with one group, of the earlier chunks'
 // entries); then every entry at its warp's running position plus its rank
 // among the warp's lanes.  Two passes: (key b, value) pairs into kv; one
-// pass: values into entries (final order).  HB: bits of the hi digit.
-template <int HB>
+// pass: values into entries (final order).  HB: bits of the hi digit; PPT:
+// points per thread.
+template <int HB, int PPT>
 __global__ void __launch_bounds__(SA_THREADS) k_sort_a_scatter(const int32_t *__restrict__ dig, SortDesc sd,
                                                                     SortParams sp, const uint32_t *__restrict__ cnt,
                                                                     uint2 *__restrict__ kv,
@@ -264,14 +269,14 @@ __global__ void __launch_bounds__(SA_THREADS) k_sort_a_scatter(const int32_t *__
     const int w1 = min(W, w0 + WC);
     for (int k = threadIdx.x; k < SORT_WARPS * GR; k += SA_THREADS) wc[k] = 0;
     __syncthreads();
-    int dg[SA_CHUNK_W][SA_PPT];
+    int dg[SA_CHUNK_W][PPT];
 #pragma unroll
     for (int j = 0; j < SA_CHUNK_W; j++) {
       const int w = w0 + j;
 #pragma unroll
-      for (int r = 0; r < SA_PPT; r++) {
-        const int q = warp * (32 * SA_PPT) + r * 32 + lane;
-        dg[j][r] = (w < w1 && q < ti.np) ? __ldg(dig + dig_index(tile, W, w, q)) : 0;
+      for (int r = 0; r < PPT; r++) {
+        const int q = warp * (32 * PPT) + r * 32 + lane;
+        dg[j][r] = (w < w1 && q < ti.np) ? __ldg(dig + dig_index(tile, W, w, q, sp.tp)) : 0;
         if (dg[j][r] != 0) {
           const int d = dg[j][r];
           const uint32_t b = (uint32_t)(d < 0 ? -d : d) - 1u;
@@ -302,8 +307,8 @@ __global__ void __launch_bounds__(SA_THREADS) k_sort_a_scatter(const int32_t *__
       if (w >= w1) break;
       const uint32_t wofs = sd.pc_stride ? (uint32_t)((int64_t)w * sd.pc_stride) : 0u;
 #pragma unroll
-      for (int r = 0; r < SA_PPT; r++) {
-        const int q = warp * (32 * SA_PPT) + r * 32 + lane;
+      for (int r = 0; r < PPT; r++) {
+        const int q = warp * (32 * PPT) + r * 32 + lane;
         const int d = dg[j][r];
         const uint32_t b = (uint32_t)(d < 0 ? -d : d) - 1u;
         const uint32_t bin = d != 0 ? (b >> shift) : 0u;
@@ -524,11 +529,14 @@ struct SortLayout {
 
   static int64_t scan_blocks(int64_t len) { return std::max<int64_t>(1, (len + SCAN_TILE - 1) / SCAN_TILE); }
 
-  // count MSMs with P points in all, tilesA pass-A tiles (ceil(size_i /
-  // SA_TP) summed over the MSMs); tabled: fixed-base window table mode.
+  // count MSMs with P points in all, tilesA pass-A tiles (ceil(size_i / tp)
+  // summed over the MSMs, tp = SA_THREADS * ppt); tabled: fixed-base window
+  // table mode.
   template <class Carver>
-  void plan(const DigitParams &dp, int count, int64_t P, int64_t tilesA, bool tabled, Carver &cv) {
+  void plan(const DigitParams &dp, int count, int64_t P, int64_t tilesA, bool tabled, Carver &cv, int ppt = SA_PPT) {
     sp.dp = dp;
+    sp.ppt = ppt;
+    sp.tp = SA_THREADS * ppt;
     sp.S = tabled ? 1 : dp.W;
     const int nb = dp.c - 1;  // bits of a bucket index
     if (nb <= 8) {
@@ -549,7 +557,7 @@ struct SortLayout {
     sp.lenA = (int64_t)sp.S * sp.RA * tilesA;
     maxM = P * dp.W;
     o_cntA = cv.template take<uint32_t>((size_t)sp.lenA + 1);
-    o_dig = cv.template take<int32_t>((size_t)tilesA * dp.W * SA_TP);
+    o_dig = cv.template take<int32_t>((size_t)tilesA * dp.W * sp.tp);
     o_bsA = cv.template take<uint32_t>((size_t)scan_blocks(sp.lenA));
     if (sp.passes == 2) {
       sp.tilesB_max = sp.NS + (maxM + SB_TILE - 1) / SB_TILE;
@@ -591,14 +599,40 @@ inline cudaError_t smem_opt_in(const void *fn, int slot, size_t bytes) {
   return e;
 }
 
-template <int HB>
+template <int HB, int PPT>
 cudaError_t launch_sort_a_scatter(cudaStream_t s, const SortParams &sp, const int32_t *dig, const SortDesc &sd,
                                   const uint32_t *cntA, uint2 *kv, uint32_t *entries) {
   const size_t sm = sort_a_smem(sp, true);
-  cudaError_t e = smem_opt_in((const void *)k_sort_a_scatter<HB>, HB, sm);
+  cudaError_t e = smem_opt_in((const void *)k_sort_a_scatter<HB, PPT>, HB, sm);
   if (e != cudaSuccess) return e;
-  k_sort_a_scatter<HB><<<(unsigned)(sp.tilesA * sort_a_blocks_per_tile(sp)), SA_THREADS, sm, s>>>(dig, sd, sp, cntA,
-                                                                                             kv, entries);
+  k_sort_a_scatter<HB, PPT><<<(unsigned)(sp.tilesA * sort_a_blocks_per_tile(sp)), SA_THREADS, sm, s>>>(
+      dig, sd, sp, cntA, kv, entries);
+  return cudaSuccess;
+}
+
+template <int PPT>
+cudaError_t launch_sort_a_scatter_hb(cudaStream_t s, const SortParams &sp, const int32_t *dig, const SortDesc &sd,
+                                     const uint32_t *cntA, uint2 *kv, uint32_t *entries) {
+  switch (sp.HB) {
+    case 1: return launch_sort_a_scatter<1, PPT>(s, sp, dig, sd, cntA, kv, entries);
+    case 2: return launch_sort_a_scatter<2, PPT>(s, sp, dig, sd, cntA, kv, entries);
+    case 3: return launch_sort_a_scatter<3, PPT>(s, sp, dig, sd, cntA, kv, entries);
+    case 4: return launch_sort_a_scatter<4, PPT>(s, sp, dig, sd, cntA, kv, entries);
+    case 5: return launch_sort_a_scatter<5, PPT>(s, sp, dig, sd, cntA, kv, entries);
+    case 6: return launch_sort_a_scatter<6, PPT>(s, sp, dig, sd, cntA, kv, entries);
+    case 7: return launch_sort_a_scatter<7, PPT>(s, sp, dig, sd, cntA, kv, entries);
+    case 8: return launch_sort_a_scatter<8, PPT>(s, sp, dig, sd, cntA, kv, entries);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <int PPT>
+cudaError_t launch_sort_a_count(cudaStream_t s, const SortParams &sp, const uint64_t *scalars, const SortDesc &sd,
+                                uint32_t *cntA, int32_t *dig) {
+  const size_t sm = sort_a_smem(sp, false);
+  cudaError_t e = smem_opt_in((const void *)k_sort_a_count<PPT>, 28 + PPT / 4, sm);
+  if (e != cudaSuccess) return e;
+  k_sort_a_count<PPT><<<(unsigned)sp.tilesA, SA_THREADS, sm, s>>>(scalars, sd, sp, cntA, dig);
   return cudaSuccess;
 }
 
@@ -612,19 +646,24 @@ cudaError_t launch_sort_b_scatter(cudaStream_t s, const SortParams &sp, const ui
   return cudaSuccess;
 }
 
-// The scatters for the digit widths of SortLayout::plan: HB in 1..8 (pass
-// A), LB in 5..11 (pass B).
+// The pass-A kernels for the tile sizes of SortLayout::plan (2, 4 or 8
+// points per thread) and the digit widths HB in 1..8; the pass-B scatter for
+// LB in 5..11.
+inline cudaError_t sort_a_count(cudaStream_t s, const SortParams &sp, const uint64_t *scalars, const SortDesc &sd,
+                                uint32_t *cntA, int32_t *dig) {
+  switch (sp.ppt) {
+    case 2: return launch_sort_a_count<2>(s, sp, scalars, sd, cntA, dig);
+    case 4: return launch_sort_a_count<4>(s, sp, scalars, sd, cntA, dig);
+    case 8: return launch_sort_a_count<8>(s, sp, scalars, sd, cntA, dig);
+    default: return cudaErrorInvalidValue;
+  }
+}
 inline cudaError_t sort_a_scatter(cudaStream_t s, const SortParams &sp, const int32_t *dig, const SortDesc &sd,
                                   const uint32_t *cntA, uint2 *kv, uint32_t *entries) {
-  switch (sp.HB) {
-    case 1: return launch_sort_a_scatter<1>(s, sp, dig, sd, cntA, kv, entries);
-    case 2: return launch_sort_a_scatter<2>(s, sp, dig, sd, cntA, kv, entries);
-    case 3: return launch_sort_a_scatter<3>(s, sp, dig, sd, cntA, kv, entries);
-    case 4: return launch_sort_a_scatter<4>(s, sp, dig, sd, cntA, kv, entries);
-    case 5: return launch_sort_a_scatter<5>(s, sp, dig, sd, cntA, kv, entries);
-    case 6: return launch_sort_a_scatter<6>(s, sp, dig, sd, cntA, kv, entries);
-    case 7: return launch_sort_a_scatter<7>(s, sp, dig, sd, cntA, kv, entries);
-    case 8: return launch_sort_a_scatter<8>(s, sp, dig, sd, cntA, kv, entries);
+  switch (sp.ppt) {
+    case 2: return launch_sort_a_scatter_hb<2>(s, sp, dig, sd, cntA, kv, entries);
+    case 4: return launch_sort_a_scatter_hb<4>(s, sp, dig, sd, cntA, kv, entries);
+    case 8: return launch_sort_a_scatter_hb<8>(s, sp, dig, sd, cntA, kv, entries);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -647,13 +686,13 @@ inline cudaError_t sort_b_scatter(cudaStream_t s, const SortParams &sp, const ui
 inline cudaError_t sort_launch(cudaStream_t s, const SortLayout &L, char *ws, const uint64_t *scalars,
                                const SortDesc &sd, int64_t K, uint32_t *offsets, uint32_t *entries, int *launches) {
   const SortParams &sp = L.sp;
-  cudaError_t e = smem_opt_in((const void *)k_sort_a_count, 0, sort_a_smem(sp, false));
-  if (e == cudaSuccess) e = smem_opt_in((const void *)k_sort_b_count, 9, sort_b_smem(sp, false));
+  cudaError_t e = smem_opt_in((const void *)k_sort_b_count, 9, sort_b_smem(sp, false));
   if (e != cudaSuccess) return e;
   auto *cntA = (uint32_t *)(ws + L.o_cntA);
   auto *bsA = (uint32_t *)(ws + L.o_bsA);
   auto *dig = (int32_t *)(ws + L.o_dig);
-  k_sort_a_count<<<(unsigned)sp.tilesA, SA_THREADS, sort_a_smem(sp, false), s>>>(scalars, sd, sp, cntA, dig);
+  e = sort_a_count(s, sp, scalars, sd, cntA, dig);
+  if (e != cudaSuccess) return e;
   scan_inplace(s, cntA, sp.lenA, bsA, launches);
   uint32_t *seg = nullptr, *tb = nullptr, *cntB = nullptr;
   if (sp.passes == 1) {

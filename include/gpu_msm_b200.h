@@ -204,6 +204,16 @@ int gm_msm_resident(gm_stream_t stream, const gm_bases *bases, int64_t base_offs
 int gm_batch_plan_create(const gm_bases *bases, int scalar_limbs, int count, const int64_t *sizes,
                          const int64_t *base_offsets, const int32_t *window_bits, gm_batch_plan **out);
 int gm_batch_plan_run(gm_batch_plan *plan, gm_stream_t stream, const uint64_t *d_scalars, void *d_results);
+/* gm_batch_plan_create with per-MSM tuning (no reference counterpart):
+ * tuning[2 i] = accumulation slices of MSM i's window class in resident waves
+ * of threads (1, 2 or 4; 0 = 1), tuning[2 i + 1] = pass-A sort tile in points
+ * per thread (2, 4 or 8, i.e. 512, 1024 or 2048 points; 0 = 4).  A class
+ * takes the values of its largest MSM.  NULL tuning = gm_batch_plan_create.
+ * The autotuner (gpu_msm_b200/autotune.py) picks them per size class. */
+int gm_batch_plan_create_tuned(const gm_bases *b, int scalar_limbs, int count, const int64_t *sizes,
+                               const int64_t *base_offsets, const int32_t *window_bits, const int32_t *tuning,
+                               gm_batch_plan **out);
+
 /* Accumulation mode of a plan (no reference counterpart): 1 (default) = the
  * accumulation of every window class in one persistent launch over a device
  * work queue of (class, 32 slices) items, between the classes' sorts and

@@ -93,6 +93,32 @@ def test_batch_mixed_window_classes(cuda):
     assert torch.equal(res_q, res)
 
 
+def test_batch_tuning_parameters_keep_results(cuda):
+    """Every (slice waves, sort tile) pair the autotuner may pick gives the
+    exact result of every MSM in both accumulation modes (the slicing changes
+    the order of the bucket sums, so the affine form is compared), and values
+    outside {1,2,4} x {2,4,8} are rejected at plan creation."""
+    import torch
+    table, logs = make_table(1 << 12, 1, cuda, seed=45)
+    sizes, offs, sc = batch_inputs(1 << 12, 20, 3, 12, seed=46)
+    wins = np.array([[5, 9][i % 2] for i in range(len(sizes))], dtype=np.int32)
+    want = expected(sizes, offs, sc, logs, 1)
+    sc_d = t_dev(sc, cuda).reshape(-1, 5)
+    for waves in (1, 2, 4):
+        for ppt in (2, 4, 8):
+            tun = np.tile(np.array([waves, ppt], dtype=np.int32), (len(sizes), 1))
+            plan = gm.BatchPlan(table, sizes, offs, window_bits=wins, tuning=tun)
+            for queue in (True, False):
+                plan.set_queue(queue)
+                res = plan.run(sc_d)
+                torch.cuda.synchronize()
+                check(res, want, 1)
+    for bad in ([3, 4], [1, 16], [-1, 4]):
+        tun = np.tile(np.array(bad, dtype=np.int32), (len(sizes), 1))
+        with pytest.raises(gm.MSMError):
+            gm.BatchPlan(table, sizes, offs, window_bits=wins, tuning=tun)
+
+
 def test_batch_graph_capture_replay(cuda):
     import torch
     table, logs = make_table(1 << 11, 1, cuda, seed=51)
