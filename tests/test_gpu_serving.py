@@ -62,15 +62,21 @@ def test_serving_results_equal_alone_and_in_mix(cuda):
 
 
 def test_serving_admission_by_memory(cuda):
-    tables, logs = _tables(cuda, n1=1 << 11, n2=1 << 9)
-    one = gm.batch_workspace_bytes(tables[1], [256])
-    budget = int(2.5 * one)
-    server = serving.MsmServer(tables, max_batch=32, max_points=1 << 12, slots=2, mem_budget=budget).start()
+    tables, logs = _tables(cuda, n1=1 << 14, n2=1 << 9)
+    # a budget that holds two 256-point requests but not three, and a request
+    # that does not fit alone (workspace sizes follow the tuned window widths,
+    # so both are derived from gm_batch_workspace_bytes)
+    budget = gm.batch_workspace_bytes(tables[1], [256, 256])
+    assert gm.batch_workspace_bytes(tables[1], [256] * 3) > budget
+    big_n = next((n for n in (1024, 2048, 4096, 8192, 16384)
+                  if gm.batch_workspace_bytes(tables[1], [n]) > budget), None)
+    assert big_n is not None
+    server = serving.MsmServer(tables, max_batch=32, max_points=1 << 14, slots=2, mem_budget=budget).start()
     reqs = []
     for i in range(12):
         sc = wl.make_scalars(256, seed=700 + i, one_frac=0.0)
         reqs.append((sc, server.submit(1, sc)))
-    big = server.submit(1, wl.make_scalars(2000, seed=799))
+    big = server.submit(1, wl.make_scalars(big_n, seed=799))
     for _, r in reqs:
         assert r.done.wait(60)
     assert big.done.wait(60)
