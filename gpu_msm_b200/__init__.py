@@ -64,7 +64,7 @@ C_API = [
     "gm_bases_create", "gm_bases_destroy", "gm_bases_count", "gm_bases_precompute", "gm_msm_resident", "gm_batch_plan_create",
     "gm_batch_plan_run", "gm_batch_plan_destroy", "gm_batch_plan_bytes", "gm_batch_plan_classes",
     "gm_batch_plan_set_queue", "gm_batch_plan_create_tuned",
-    "gm_batch_run", "gm_batch_workspace_bytes", "gm_g1_sum_projective_host",
+    "gm_batch_run", "gm_batch_workspace_bytes", "gm_g1_sum_projective_host", "gm_batch_run_ws",
     "gm_host_selftest", "gm_fp_elem", "gm_fp2_elem", "gm_g1_point_elem", "gm_g2_point_elem",
     "gm_g1_on_curve_batch", "gm_g2_on_curve_batch", "gm_g1_msm_host_async", "gm_g2_msm_host_async",
 ]
@@ -128,6 +128,7 @@ def lib() -> ctypes.CDLL:
         L.gm_batch_plan_set_queue.argtypes = [vp, i32]
         L.gm_batch_plan_create_tuned.argtypes = [vp, i32, i32, vp, vp, vp, vp, vp]
         L.gm_batch_run.argtypes = [vp, vp, i32, i32, vp, vp, vp, vp, vp]
+        L.gm_batch_run_ws.argtypes = [vp, vp, i32, i32, vp, vp, vp, vp, vp, vp, i64]
         L.gm_g1_sum_projective_host.argtypes = [vp, vp, i32]
         L.gm_batch_workspace_bytes.argtypes = [vp, i32, i32, vp, vp]
         L.gm_batch_workspace_bytes.restype = i64
@@ -773,10 +774,13 @@ class BatchPlan:
             pass
 
 
-def batch_run(bases: ResidentBases, sizes, scalars, base_offsets=None, window_bits=None, out=None, stream=None):
-    """One batch without a plan (``gm_batch_run``): workspace from the stream-
-    ordered pool, classes in order on the stream.  For batches whose shape
-    changes on every call."""
+def batch_run(bases: ResidentBases, sizes, scalars, base_offsets=None, window_bits=None, out=None, stream=None,
+              workspace=None):
+    """One batch without a plan (``gm_batch_run``): classes in order on the
+    stream, for batches whose shape changes on every call.  workspace: None
+    takes the device memory from the library's stream-ordered pool for this
+    run; or a uint8 device tensor of at least ``batch_workspace_bytes`` bytes
+    (``gm_batch_run_ws``), in use until the stream has run the batch."""
     import torch
     sizes = np.ascontiguousarray(sizes, dtype=np.int64)
     total = int(sizes.sum())
@@ -788,9 +792,16 @@ def batch_run(bases: ResidentBases, sizes, scalars, base_offsets=None, window_bi
     words = G1P_WORDS if bases.group == 1 else G2P_WORDS
     if out is None:
         out = torch.empty((len(sizes), words), dtype=torch.int64, device=scalars.device)
-    _check(lib().gm_batch_run(_stream_handle(stream), bases.handle, scalars.shape[1], len(sizes), _p(sizes),
-                              None if offs is None else _p(offs), _p(wins), ctypes.c_void_p(scalars.data_ptr()),
-                              ctypes.c_void_p(out.data_ptr())), "gm_batch_run")
+    args = (_stream_handle(stream), bases.handle, scalars.shape[1], len(sizes), _p(sizes),
+            None if offs is None else _p(offs), _p(wins), ctypes.c_void_p(scalars.data_ptr()),
+            ctypes.c_void_p(out.data_ptr()))
+    if workspace is None:
+        _check(lib().gm_batch_run(*args), "gm_batch_run")
+    else:
+        if workspace.dtype != torch.uint8 or workspace.device != scalars.device:
+            raise ValueError("workspace: uint8 tensor on the scalars' device")
+        _check(lib().gm_batch_run_ws(*args, ctypes.c_void_p(workspace.data_ptr()), workspace.numel()),
+               "gm_batch_run_ws")
     return out
 
 

@@ -6,6 +6,7 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/gpu_msm_b200.h"
@@ -241,6 +242,10 @@ __global__ void k_proj_sum(uint64_t *__restrict__ out, const uint64_t *__restric
   gm::store_ref<F>(out + 2 * Hw, Z);
 }
 
+// host arithmetic of a device field: gm::Fp -> gm_host::F1, gm::Fp2 -> F2
+template <class F>
+using HostField = typename std::conditional<sizeof(typename F::T) == sizeof(gm::fp_t), gm_host::F1, gm_host::F2>::type;
+
 template <class F, class Aff, class Prj>
 int host_msm(Prj *result, const Aff *points, const uint64_t *scalars, int limbs, int n, uint32_t gpu_index,
              int to_mont) {
@@ -276,9 +281,20 @@ int host_msm(Prj *result, const Aff *points, const uint64_t *scalars, int limbs,
   const size_t o_res = o_sc + (sc_bytes + 255) / 256 * 256;
   const size_t o_err = o_res + 512;
   char *buf = nullptr;
-  uint32_t err_host = 0;
+  // the window sums come back to this thread, which runs the Horner tail
+  // itself: no stream host function and no result copy in and out
+  void *slot = nullptr;
+  uint32_t *err_host = nullptr;
+  gm::TailHandoff handoff;
   cudaError_t e = cudaSuccess;
-  rc = gm::pool_alloc((int)gpu_index, s, o_err + 256, (void **)&buf);
+  rc = gm::pinned_acquire(&slot);
+  if (rc == gm::GM_OK) {
+    err_host = static_cast<uint32_t *>(slot);
+    *err_host = 0;
+    handoff.host = static_cast<char *>(slot) + 256;
+    handoff.cap = gm::PINNED_SLOT_BYTES - 256;
+    rc = gm::pool_alloc((int)gpu_index, s, o_err + 256, (void **)&buf);
+  }
   if (rc == gm::GM_OK) {
     e = cudaMemcpyAsync(buf + o_sc, scalars, sc_bytes, cudaMemcpyHostToDevice, s);
     // the points' stream may use the buffer once its allocation is ordered
@@ -289,12 +305,8 @@ int host_msm(Prj *result, const Aff *points, const uint64_t *scalars, int limbs,
     if (e == cudaSuccess) {
       rc = gm::msm_launch<F>(s, (int)gpu_index, nullptr, (const uint64_t *)buf, to_mont,
                              (const uint64_t *)(buf + o_sc), limbs, n, (uint64_t *)(buf + o_res), 0,
-                             (uint32_t *)(buf + o_err), pts_done);
-      if (rc == gm::GM_OK) {
-        e = cudaMemcpyAsync(result, buf + o_res, sizeof(Prj), cudaMemcpyDeviceToHost, s);
-        if (e == cudaSuccess)
-          e = cudaMemcpyAsync(&err_host, buf + o_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
-      }
+                             (uint32_t *)(buf + o_err), pts_done, &handoff);
+      if (rc == gm::GM_OK) e = cudaMemcpyAsync(err_host, buf + o_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
     }
     // s waited for pts_done inside msm_launch, or waits here on an early error
     cudaStreamWaitEvent(s, pts_done, 0);
@@ -306,11 +318,17 @@ int host_msm(Prj *result, const Aff *points, const uint64_t *scalars, int limbs,
   cudaEventDestroy(pts_done);
   cudaStreamDestroy(s);
   cudaStreamDestroy(s2);
+  const uint32_t flag = err_host ? *err_host : 0u;
+  if (rc == gm::GM_OK && e == cudaSuccess && se == cudaSuccess && se2 == cudaSuccess && flag == 0)
+    gm_host::horner_to_proj<HostField<F>>(reinterpret_cast<uint64_t *>(result),
+                                          reinterpret_cast<const gm_host::HXyzz<HostField<F>> *>(handoff.host),
+                                          handoff.W, handoff.c);
+  if (slot) gm::pinned_release(slot);
   if (rc) return rc;
   if (e != cudaSuccess) return gm::record_error(e, "host_msm copy");
   if (se != cudaSuccess) return gm::record_error(se, "host_msm sync");
   if (se2 != cudaSuccess) return gm::record_error(se2, "host_msm sync");
-  if (err_host) return gm::GM_ERR_CHECK;
+  if (flag) return gm::GM_ERR_CHECK;
   return gm::GM_OK;
 }
 

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdint>
 #include <cstring>
 #include <map>
 #include <new>
@@ -15,9 +16,9 @@
 namespace gm {
 // heavy templates are instantiated once, in msm_g1.cu / msm_g2.cu
 extern template int msm_launch<Fp>(cudaStream_t, int, const uint4 *, const uint64_t *, int, const uint64_t *, int,
-                                   int64_t, uint64_t *, int, uint32_t *, cudaEvent_t);
+                                   int64_t, uint64_t *, int, uint32_t *, cudaEvent_t, TailHandoff *);
 extern template int msm_launch<Fp2>(cudaStream_t, int, const uint4 *, const uint64_t *, int, const uint64_t *, int,
-                                    int64_t, uint64_t *, int, uint32_t *, cudaEvent_t);
+                                    int64_t, uint64_t *, int, uint32_t *, cudaEvent_t, TailHandoff *);
 extern template int batch_layouts<Fp>(BatchPlan &, int);
 extern template int batch_layouts<Fp2>(BatchPlan &, int);
 extern template int batch_run<Fp>(const BatchPlan &, cudaStream_t, const uint64_t *, uint64_t *);
@@ -379,9 +380,11 @@ int64_t gm_batch_workspace_bytes(const gm_bases *b, int scalar_limbs, int count,
   return bytes;
 }
 
-int gm_batch_run(gm_stream_t stream, const gm_bases *b, int scalar_limbs, int count, const int64_t *sizes,
-                 const int64_t *base_offsets, const int32_t *window_bits, const uint64_t *d_scalars,
-                 void *d_results) {
+// gm_batch_run / gm_batch_run_ws: ws == nullptr takes the workspace from the
+// stream-ordered pool for this run; otherwise the caller's ws_bytes at ws.
+static int batch_run_once(gm_stream_t stream, const gm_bases *b, int scalar_limbs, int count, const int64_t *sizes,
+                   const int64_t *base_offsets, const int32_t *window_bits, const uint64_t *d_scalars,
+                   void *d_results, void *ws, size_t ws_bytes) {
   if (!d_scalars || !d_results) return gm::GM_ERR_ARG;
   gm::BatchPlan plan;
   std::vector<std::vector<int64_t>> d64;
@@ -403,8 +406,16 @@ int gm_batch_run(gm_stream_t stream, const gm_bases *b, int scalar_limbs, int co
     total += (plan.classes[k].ws_bytes + 255) / 256 * 256;
   }
   char *mem = nullptr;
-  rc = gm::pool_alloc(plan.dev, s, total, (void **)&mem);
-  if (rc) return rc;
+  if (ws) {
+    if (total > ws_bytes || (reinterpret_cast<uintptr_t>(ws) & 255u)) {
+      gm::set_last_error("batch workspace too small or not 256-byte aligned");
+      return gm::GM_ERR_ARG;
+    }
+    mem = static_cast<char *>(ws);
+  } else {
+    rc = gm::pool_alloc(plan.dev, s, total, (void **)&mem);
+    if (rc) return rc;
+  }
   // descriptors go through one pinned slot (an asynchronous copy from pageable
   // memory would first wait for the stream), released in stream order
   void *slot = nullptr;
@@ -426,15 +437,30 @@ int gm_batch_run(gm_stream_t stream, const gm_bases *b, int scalar_limbs, int co
     }
     if (e != cudaSuccess) {
       if (pinned) gm::enqueue_pinned_release(s, slot);
-      cudaFreeAsync(mem, s);
+      if (!ws) cudaFreeAsync(mem, s);
       return gm::record_error(e, "batch descriptors");
     }
   }
   if (pinned) gm::enqueue_pinned_release(s, slot);
   rc = plan.group == 1 ? gm::batch_run<gm::Fp>(plan, s, d_scalars, (uint64_t *)d_results)
                        : gm::batch_run<gm::Fp2>(plan, s, d_scalars, (uint64_t *)d_results);
-  cudaFreeAsync(mem, s);
+  if (!ws) cudaFreeAsync(mem, s);
   return rc;
+}
+
+int gm_batch_run(gm_stream_t stream, const gm_bases *b, int scalar_limbs, int count, const int64_t *sizes,
+                 const int64_t *base_offsets, const int32_t *window_bits, const uint64_t *d_scalars,
+                 void *d_results) {
+  return batch_run_once(stream, b, scalar_limbs, count, sizes, base_offsets, window_bits, d_scalars, d_results,
+                        nullptr, 0);
+}
+
+int gm_batch_run_ws(gm_stream_t stream, const gm_bases *b, int scalar_limbs, int count, const int64_t *sizes,
+                    const int64_t *base_offsets, const int32_t *window_bits, const uint64_t *d_scalars,
+                    void *d_results, void *d_workspace, int64_t workspace_bytes) {
+  if (!d_workspace || workspace_bytes <= 0) return gm::GM_ERR_ARG;
+  return batch_run_once(stream, b, scalar_limbs, count, sizes, base_offsets, window_bits, d_scalars, d_results,
+                        d_workspace, (size_t)workspace_bytes);
 }
 
 int gm_batch_plan_run(gm_batch_plan *p, gm_stream_t stream, const uint64_t *d_scalars, void *d_results) {

@@ -49,15 +49,27 @@ int64_t launches_and_reset();
 int pool_alloc(int dev, cudaStream_t s, size_t bytes, void **ptr);
 int default_window(int group, int64_t n, int limbs);
 
+// Window sums handed to a synchronous caller in place of the stream-ordered
+// host tail: the MSM copies its W window sums (XYZZ, device layout) to
+// `host` (pinned, `cap` bytes), sets W and c and writes no result; the caller
+// combines them (gm_host::horner_to_proj) after synchronising the stream.
+struct TailHandoff {
+  void *host = nullptr;
+  size_t cap = 0;
+  int W = 0, c = 0;
+};
+
 // Full MSM pipeline on `s`.  Either `bases` (packed records) or `ref_points`
 // (reference-layout affine points; converted to Montgomery when to_mont) is
 // given.  Writes the projective result (reference layout) to out_proj.  When
 // err_out is non-null it receives the device consistency flag (0 = ok).
 // bases_ready (optional): an event the stream waits for after the sort,
 // before the bases are first read (the sort reads only the scalars).
+// handoff (optional, not while capturing): the window sums go to the caller
+// instead of a result in out_proj.
 template <class F>
 int msm_launch(cudaStream_t s, int dev, const uint4 *bases, const uint64_t *ref_points, int to_mont,
                const uint64_t *scalars, int limbs, int64_t n, uint64_t *out_proj, int c_override, uint32_t *err_out,
-               cudaEvent_t bases_ready = nullptr);
+               cudaEvent_t bases_ready = nullptr, TailHandoff *handoff = nullptr);
 
 }  // namespace gm

@@ -265,11 +265,12 @@ int msm_plan(MsmLayout<F> &lay, int dev, int64_t n, int limbs, int c, bool pack,
 // always while s is being captured, on the device.  err_out (optional,
 // device) receives the consistency flag of the fix-up (0 = ok).  bases_ready
 // (optional): an event the stream waits for after the sort, before the bases
-// are first read.
+// are first read.  handoff (optional): the window sums are copied to the
+// caller's pinned buffer instead, and out_proj is not written.
 template <class F>
 int msm_run(cudaStream_t s, const MsmLayout<F> &lay, char *ws, const uint4 *bases, const uint64_t *ref_points,
             int to_mont, const uint64_t *scalars, uint64_t *out_proj, bool host_tail, uint32_t *err_out,
-            cudaEvent_t bases_ready) {
+            cudaEvent_t bases_ready, TailHandoff *handoff = nullptr) {
   constexpr int H = F::LIMBS / 2;  // u64 words per coordinate
   const int64_t n = lay.n;
   auto *offsets = (uint32_t *)(ws + lay.o_offsets);
@@ -323,7 +324,20 @@ int msm_run(cudaStream_t s, const MsmLayout<F> &lay, char *ws, const uint4 *base
   // latency per product) unless the stream is being captured into a graph
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   GM_CHECK(cudaStreamIsCapturing(s, &cap));
-  if (host_tail && cap == cudaStreamCaptureStatusNone) {
+  if (handoff && cap != cudaStreamCaptureStatusNone) {
+    set_last_error("window-sum handoff while the stream is being captured");
+    return GM_ERR_ARG;
+  }
+  if (handoff) {
+    const size_t bytes = (size_t)W * sizeof(xyzz_t<F>);
+    if (bytes > handoff->cap) {
+      set_last_error("window-sum handoff buffer too small");
+      return GM_ERR_ARG;
+    }
+    GM_CHECK(cudaMemcpyAsync(handoff->host, src, bytes, cudaMemcpyDeviceToHost, s));
+    handoff->W = W;
+    handoff->c = lay.dp.c;
+  } else if (host_tail && cap == cudaStreamCaptureStatusNone) {
     rc = enqueue_host_tail(s, F::LIMBS == NL ? 1 : 2, src, W, lay.dp.c, out_proj);
     if (rc) return rc;
   } else {
@@ -343,7 +357,7 @@ int msm_run(cudaStream_t s, const MsmLayout<F> &lay, char *ws, const uint4 *base
 template <class F>
 int msm_launch(cudaStream_t s, int dev, const uint4 *bases, const uint64_t *ref_points, int to_mont,
                const uint64_t *scalars, int limbs, int64_t n, uint64_t *out_proj, int c_override,
-               uint32_t *err_out, cudaEvent_t bases_ready) {
+               uint32_t *err_out, cudaEvent_t bases_ready, TailHandoff *handoff) {
   constexpr int H = F::LIMBS / 2;
   if (n == 0) {
     if (err_out) GM_CHECK(cudaMemsetAsync(err_out, 0, sizeof(uint32_t), s));
@@ -358,7 +372,7 @@ int msm_launch(cudaStream_t s, int dev, const uint4 *bases, const uint64_t *ref_
   rc = pool_alloc(dev, s, lay.bytes, (void **)&ws);
   if (rc) return rc;
   rc = msm_run<F>(s, lay, ws, bases, ref_points, to_mont, scalars, out_proj, host_tail_enabled(), err_out,
-                  bases_ready);
+                  bases_ready, handoff);
   const cudaError_t e = cudaFreeAsync(ws, s);
   if (rc) return rc;
   return e == cudaSuccess ? GM_OK : record_error(e, "cudaFreeAsync(workspace)");

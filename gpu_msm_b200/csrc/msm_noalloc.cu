@@ -38,7 +38,7 @@ namespace gm {
 // instantiated once, in msm_g1.cu
 extern template int msm_plan<Fp>(MsmLayout<Fp> &, int, int64_t, int, int, bool, int64_t);
 extern template int msm_run<Fp>(cudaStream_t, const MsmLayout<Fp> &, char *, const uint4 *, const uint64_t *, int,
-                                const uint64_t *, uint64_t *, bool, uint32_t *, cudaEvent_t);
+                                const uint64_t *, uint64_t *, bool, uint32_t *, cudaEvent_t, TailHandoff *);
 }  // namespace gm
 
 namespace {

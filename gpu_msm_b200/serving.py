@@ -14,11 +14,15 @@ through pinned memory.  Requests that arrive while batches run wait in the
 queue and are admitted as soon as a slot and memory free up, so their work
 overlaps with batches already on the device.
 
-Admission by free device memory: at start the server measures the free device
-memory and keeps ``budget = free - reserve``; a batch is admitted only if its
-workspace (``gm_batch_workspace_bytes``) plus the bytes of the batches in
-flight fit the budget.  A single request that cannot fit even alone is
-rejected with an error.
+Admission by device memory: at start the server measures the free device
+memory and keeps ``budget = free - reserve``.  Every slot owns a fixed device
+workspace of ``slot_bytes`` (by default twice the largest workspace of a
+batch at the server's limits, and at most budget / slots), allocated once, and
+runs its batches in it (``gm_batch_run_ws``): no batch takes an allocation
+from the library's stream-ordered pool, whose growth under load was measured
+to stall a launch for up to a second.  A batch is admitted only if its
+workspace (``gm_batch_workspace_bytes``) fits a slot; a single request that
+cannot fit even alone is rejected with an error.
 
 Latency of a request = completion time - submission time (host clock); the
 server records both for p50/p99.
@@ -60,6 +64,7 @@ class _Slot:
         self.d_sc = torch.empty((max_points, limbs), dtype=torch.int64, device=dev)
         self.d_out = torch.empty(max_batch * gm.G2P_WORDS, dtype=torch.int64, device=dev)
         self.h_out = torch.empty(max_batch * gm.G2P_WORDS, dtype=torch.int64, pin_memory=True)
+        self.ws = None
         self.event = None
         self.reqs = []
         self.bytes = 0
@@ -68,7 +73,7 @@ class _Slot:
 
 class MsmServer:
     def __init__(self, tables: dict, max_batch: int = 64, max_points: int = 1 << 22, slots: int = 2,
-                 mem_reserve: int = 2 << 30, mem_budget: int = None, scalar_limbs: int = 5):
+                 mem_reserve: int = 2 << 30, mem_budget: int = None, scalar_limbs: int = 5, slot_bytes: int = None):
         import torch
         self.torch = torch
         self.tables = tables
@@ -79,6 +84,13 @@ class MsmServer:
         free, _ = torch.cuda.mem_get_info(self.dev)
         self.budget = mem_budget if mem_budget is not None else max(0, free - mem_reserve)
         self.slots = [_Slot(torch, self.dev, max_points, scalar_limbs, max_batch) for _ in range(slots)]
+        if slot_bytes is None:
+            need = max((gm.batch_workspace_bytes(t, sz, scalar_limbs=scalar_limbs) for _, t, sz in self._limit_shapes()),
+                       default=0)
+            slot_bytes = min(self.budget // max(1, slots), 2 * need)
+        self.slot_bytes = int(slot_bytes) // 256 * 256
+        for sl in self.slots:
+            sl.ws = torch.empty(max(256, self.slot_bytes), dtype=torch.uint8, device=self.dev)
         self.pending = collections.deque()
         self.cv = threading.Condition()
         self.stop_flag = False
@@ -103,7 +115,17 @@ class MsmServer:
             self.cv.notify()
         return r
 
-    def start(self):
+    def start(self, warmup: bool = True):
+        """Start the worker thread.  warmup: first run, on every slot at once,
+        batches of each group at the server's limits (one MSM of max_points,
+        and max_batch MSMs sharing max_points) with zero scalars.  Their
+        workspaces and kernels are those of real batches, so the library's
+        stream-ordered memory pool already holds the memory of concurrent
+        batches and every kernel is loaded: no request waits for the pool to
+        grow (tens of milliseconds, occasionally far more, under load) or for a
+        first launch."""
+        if warmup:
+            self._warmup()
         self.stop_flag = False
         self.thread = threading.Thread(target=self._loop, name="msm-server", daemon=True)
         self.thread.start()
@@ -120,8 +142,30 @@ class MsmServer:
             self.thread = None
 
     # ---------------------------------------------------------------- worker
-    def _in_flight_bytes(self):
-        return sum(s.bytes for s in self.slots if s.event is not None)
+    def _limit_shapes(self):
+        """(group, table, sizes) of batches at the server's limits: the
+        largest requests the table allows, as many as max_points holds, and
+        max_batch equal requests sharing max_points."""
+        for group, table in self.tables.items():
+            n = min(self.max_points, table.n)
+            yield group, table, [n] * max(1, min(self.max_batch, self.max_points // n))
+            per = max(1, min(n, self.max_points // self.max_batch))
+            yield group, table, [per] * max(1, min(self.max_batch, self.max_points // per))
+
+    def _warmup(self):
+        torch = self.torch
+        for group, table, sizes in self._limit_shapes():
+            if gm.batch_workspace_bytes(table, sizes, scalar_limbs=self.limbs) > self.slot_bytes:
+                continue
+            words = gm.G1P_WORDS if group == 1 else gm.G2P_WORDS
+            total = int(sum(sizes))
+            for slot in self.slots:
+                with torch.cuda.stream(slot.stream):
+                    slot.d_sc[:total].zero_()
+                    out = slot.d_out[:len(sizes) * words].view(len(sizes), words)
+                    gm.batch_run(table, sizes, slot.d_sc[:total], out=out, stream=slot.stream, workspace=slot.ws)
+            for slot in self.slots:
+                slot.stream.synchronize()
 
     def _reap(self):
         """Complete the slots whose batch finished."""
@@ -149,7 +193,6 @@ class MsmServer:
         group = self.pending[0].group
         table = self.tables[group]
         take, sizes, points = [], [], 0
-        avail = self.budget - self._in_flight_bytes()
         for r in list(self.pending):
             if r.group != group:
                 continue
@@ -158,9 +201,9 @@ class MsmServer:
                 break
             trial = sizes + [n]
             need = gm.batch_workspace_bytes(table, trial, scalar_limbs=self.limbs)
-            if need > avail:
-                if not take and self._in_flight_bytes() == 0:
-                    # cannot fit even alone on an idle device
+            if need > self.slot_bytes:
+                if not take:
+                    # cannot fit even alone in a slot's workspace
                     self.pending.remove(r)
                     r.error = "request does not fit the device-memory budget"
                     r.t_done = time.perf_counter()
@@ -191,7 +234,7 @@ class MsmServer:
             slot.d_sc[:total].copy_(slot.h_sc[:total], non_blocking=True)
             out = slot.d_out[:len(reqs) * words].view(len(reqs), words)
             gm.batch_run(self.tables[group], sizes, slot.d_sc[:total], base_offsets=offs, out=out,
-                         stream=slot.stream)
+                         stream=slot.stream, workspace=slot.ws)
             slot.h_out[:len(reqs) * words].copy_(slot.d_out[:len(reqs) * words], non_blocking=True)
             ev = torch.cuda.Event()
             ev.record(slot.stream)

@@ -181,6 +181,12 @@ int gm_g1_msm_device_noalloc(gm_stream_t stream, uint32_t gpu_index, G1Projectiv
  *   from the per-device stream-ordered pool for this one run and the classes
  *   run in order on `stream` (for batches whose shape changes every time, as
  *   in serving).
+ * gm_batch_run_ws: gm_batch_run in the caller's device workspace
+ *   (d_workspace, 256-byte aligned, workspace_bytes at least
+ *   gm_batch_workspace_bytes of the batch; GM_ERR_ARG otherwise), so that a
+ *   server that keeps one workspace per in-flight batch takes no pool
+ *   allocation per batch.  The workspace is in use until the stream has run
+ *   the batch.  No counterpart in the reference.
  * gm_batch_workspace_bytes: device bytes gm_batch_run takes for that batch
  *   (for admission control), or -1 on a bad argument. */
 typedef struct gm_bases gm_bases;
@@ -226,6 +232,9 @@ int64_t gm_batch_plan_bytes(const gm_batch_plan *plan);
 int gm_batch_plan_classes(const gm_batch_plan *plan, int32_t *window_bits, int32_t *counts, int max);
 int gm_batch_run(gm_stream_t stream, const gm_bases *bases, int scalar_limbs, int count, const int64_t *sizes,
                  const int64_t *base_offsets, const int32_t *window_bits, const uint64_t *d_scalars, void *d_results);
+int gm_batch_run_ws(gm_stream_t stream, const gm_bases *bases, int scalar_limbs, int count, const int64_t *sizes,
+                    const int64_t *base_offsets, const int32_t *window_bits, const uint64_t *d_scalars,
+                    void *d_results, void *d_workspace, int64_t workspace_bytes);
 int64_t gm_batch_workspace_bytes(const gm_bases *bases, int scalar_limbs, int count, const int64_t *sizes,
                                  const int32_t *window_bits);
 

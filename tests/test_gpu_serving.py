@@ -63,15 +63,16 @@ def test_serving_results_equal_alone_and_in_mix(cuda):
 
 def test_serving_admission_by_memory(cuda):
     tables, logs = _tables(cuda, n1=1 << 14, n2=1 << 9)
-    # a budget that holds two 256-point requests but not three, and a request
-    # that does not fit alone (workspace sizes follow the tuned window widths,
-    # so both are derived from gm_batch_workspace_bytes)
-    budget = gm.batch_workspace_bytes(tables[1], [256, 256])
-    assert gm.batch_workspace_bytes(tables[1], [256] * 3) > budget
+    # slot workspaces that hold two 256-point requests but not three, and a
+    # request that does not fit alone (workspace sizes follow the tuned window
+    # widths, so both are derived from gm_batch_workspace_bytes)
+    slot = gm.batch_workspace_bytes(tables[1], [256, 256])
+    assert gm.batch_workspace_bytes(tables[1], [256] * 3) > slot
     big_n = next((n for n in (1024, 2048, 4096, 8192, 16384)
-                  if gm.batch_workspace_bytes(tables[1], [n]) > budget), None)
+                  if gm.batch_workspace_bytes(tables[1], [n]) > slot), None)
     assert big_n is not None
-    server = serving.MsmServer(tables, max_batch=32, max_points=1 << 14, slots=2, mem_budget=budget).start()
+    server = serving.MsmServer(tables, max_batch=32, max_points=1 << 14, slots=2, slot_bytes=slot).start()
+    assert server.slot_bytes <= slot
     reqs = []
     for i in range(12):
         sc = wl.make_scalars(256, seed=700 + i, one_frac=0.0)
@@ -82,7 +83,7 @@ def test_serving_admission_by_memory(cuda):
     assert big.done.wait(60)
     server.stop()
     g1_batches = [b for b in server.batches if b[1] == 1]
-    assert max(b[2] for b in g1_batches) <= 2, "a batch exceeded the memory budget"
+    assert max(b[2] for b in g1_batches) <= 2, "a batch exceeded its slot's workspace"
     assert big.error is not None and "budget" in big.error
     for sc, r in reqs:
         want = oracle.generator_multiple(wl.expected_log(sc, logs[1][:len(sc)]), group=1)
