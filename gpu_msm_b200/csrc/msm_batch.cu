@@ -198,6 +198,18 @@ int build_classes(const gm_bases *b, int scalar_limbs, int count, const int64_t 
 
 }  // namespace
 
+// Device bytes of a transient batch (descriptors and workspaces of every
+// class, each 256-byte aligned): the figure gm_batch_workspace_bytes reports
+// and gm_batch_run_ws requires.
+static int64_t transient_bytes(const gm::BatchPlan &plan, const std::vector<std::vector<int64_t>> &d64,
+                               const std::vector<std::vector<int32_t>> &idx) {
+  int64_t bytes = 0;
+  for (size_t k = 0; k < plan.classes.size(); k++)
+    bytes += (int64_t)(plan.classes[k].ws_bytes + d64[k].size() * sizeof(int64_t) + idx[k].size() * sizeof(int32_t) +
+                       512);
+  return bytes;
+}
+
 extern "C" {
 
 int gm_bases_create(uint32_t gpu_index, int group, const void *d_points, int64_t n, int points_montgomery,
@@ -373,11 +385,7 @@ int64_t gm_batch_workspace_bytes(const gm_bases *b, int scalar_limbs, int count,
   std::vector<std::vector<int64_t>> d64;
   std::vector<std::vector<int32_t>> idx;
   if (build_classes(b, scalar_limbs, count, sizes, nullptr, window_bits, plan, d64, idx)) return -1;
-  int64_t bytes = 0;
-  for (size_t k = 0; k < plan.classes.size(); k++)
-    bytes += (int64_t)(plan.classes[k].ws_bytes + d64[k].size() * sizeof(int64_t) + idx[k].size() * sizeof(int32_t) +
-                       512);
-  return bytes;
+  return transient_bytes(plan, d64, idx);
 }
 
 // gm_batch_run / gm_batch_run_ws: ws == nullptr takes the workspace from the
@@ -407,7 +415,8 @@ static int batch_run_once(gm_stream_t stream, const gm_bases *b, int scalar_limb
   }
   char *mem = nullptr;
   if (ws) {
-    if (total > ws_bytes || (reinterpret_cast<uintptr_t>(ws) & 255u)) {
+    if (total > ws_bytes || (size_t)transient_bytes(plan, d64, idx) > ws_bytes ||
+        (reinterpret_cast<uintptr_t>(ws) & 255u)) {
       gm::set_last_error("batch workspace too small or not 256-byte aligned");
       return gm::GM_ERR_ARG;
     }

@@ -145,6 +145,37 @@ def test_batch_graph_capture_replay(cuda):
     del g
 
 
+def test_batch_run_in_caller_workspace(cuda):
+    """gm_batch_run_ws: the transient batch in a caller-owned workspace of
+    gm_batch_workspace_bytes gives the exact results, the same words as the
+    pooled gm_batch_run, and the workspace is reusable right away on the
+    same stream; a workspace one byte short, or not 256-byte aligned, is
+    refused before anything is enqueued."""
+    import torch
+    table, logs = make_table(1 << 11, 1, cuda, seed=47)
+    table.precompute(8)
+    sizes, offs, sc = batch_inputs(1 << 11, 18, 2, 11, seed=48)
+    wins = np.array([[0, 5, 9][i % 3] for i in range(len(sizes))], dtype=np.int32)
+    need = gm.batch_workspace_bytes(table, sizes, window_bits=wins)
+    ws = torch.empty(need, dtype=torch.uint8, device=cuda)
+    sc_d = t_dev(sc, cuda).reshape(-1, 5)
+    want = expected(sizes, offs, sc, logs, 1)
+    pooled = gm.batch_run(table, sizes, sc_d, base_offsets=offs, window_bits=wins)
+    own = gm.batch_run(table, sizes, sc_d, base_offsets=offs, window_bits=wins, workspace=ws)
+    torch.cuda.synchronize()
+    check(own, want, 1)
+    assert torch.equal(own, pooled)
+    sc2 = wl.make_scalars(int(sizes.sum()), seed=49)
+    again = gm.batch_run(table, sizes, t_dev(sc2, cuda).reshape(-1, 5), base_offsets=offs, window_bits=wins,
+                         workspace=ws)
+    torch.cuda.synchronize()
+    check(again, expected(sizes, offs, sc2, logs, 1), 1)
+    with pytest.raises(gm.MSMError):
+        gm.batch_run(table, sizes, sc_d, base_offsets=offs, window_bits=wins, workspace=ws[:need - 1])
+    with pytest.raises(gm.MSMError):
+        gm.batch_run(table, sizes, sc_d, base_offsets=offs, window_bits=wins, workspace=ws[16:])
+
+
 def test_batch_g2(cuda):
     import torch
     table, logs = make_table(1 << 9, 2, cuda, seed=61)
