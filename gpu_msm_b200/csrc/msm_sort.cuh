@@ -202,10 +202,26 @@ GM_DEVI void tile_digits(const uint64_t *sc, const TileA &ti, const SortParams &
   }
 }
 
+// The tile's scalar words into shared memory with coalesced 128-bit loads
+// from the first 16-byte boundary of the tile's rows (scalar rows are 8-byte
+// aligned; with 5 limbs every other tile starts in the middle of a 16-byte
+// pair); a leading and a trailing odd word take 64-bit loads.
 GM_DEVI void stage_scalars(uint64_t *sc, const uint64_t *scalars, const TileA &ti, int limbs) {
   const uint64_t *src = scalars + ti.sc_row * limbs;
   const int64_t words = ti.np * limbs;
-  for (int64_t k = threadIdx.x; k < words; k += SA_THREADS) sc[k] = __ldg(src + k);
+  if (words <= 0) return;
+  const int head = (int)((reinterpret_cast<uintptr_t>(src) >> 3) & 1u);  // src is 8 mod 16
+  const int64_t body = words - head;                                       // >= 0
+  if (threadIdx.x == 0) {
+    if (head) sc[0] = __ldg(src);
+    if (body & 1) sc[words - 1] = __ldg(src + words - 1);
+  }
+  const uint4 *src4 = reinterpret_cast<const uint4 *>(src + head);
+  for (int64_t k = threadIdx.x; k < (body >> 1); k += SA_THREADS) {
+    const uint4 v = __ldg(src4 + k);
+    sc[head + 2 * k] = (uint64_t)v.x | ((uint64_t)v.y << 32);
+    sc[head + 2 * k + 1] = (uint64_t)v.z | ((uint64_t)v.w << 32);
+  }
 }
 
 // Pass A, counting: the tile's signed digits (into dig) and its entries per
