@@ -86,7 +86,7 @@ def test_elem_rejects_bad_arguments(cuda):
 def test_on_curve_batch(cuda, group):
     """Batched on-curve check with the constants the generators satisfy
     (b = 1, b' = 1 + i): multiples of G pass, infinity passes, points with a
-    perturbed coordinate fail; the verdicts equal the oracle's."""
+    perturbed coordinate fail; the answers equal the oracle's."""
     from gpu_msm_b200 import workload as wl
     from oracle import pyref as pr
     n = 300
