@@ -314,7 +314,7 @@ def run_ours(args, rank, world, local_rank):
     # one result (and gather) buffer per stream, so that MSMs in flight on
     # different streams never share one
     outs = [torch.empty(gm.G1P_WORDS, dtype=torch.int64, device=dev) for _ in range(PIPELINE_STREAMS)]
-    gathered = [torch.empty((world, gm.G1P_WORDS), dtype=torch.int64, device=dev) if world > 1 else None
+    gathered = [torch.empty(world * gm.G1P_WORDS, dtype=torch.int64, device=dev) if world > 1 else None
                 for _ in range(PIPELINE_STREAMS)]
 
     def step(k, stream):
@@ -322,7 +322,7 @@ def run_ours(args, rank, world, local_rank):
             gm.msm_device(pts_d, sc_d, group=1, out=outs[k], stream=stream)
             if world > 1:
                 dist.all_gather_into_tensor(gathered[k], outs[k])
-                gm.sum_projective(gathered[k], group=1, out=outs[k], stream=stream)
+                gm.sum_projective(gathered[k].view(world, gm.G1P_WORDS), group=1, out=outs[k], stream=stream)
 
     main = torch.cuda.current_stream()
     side = [torch.cuda.Stream() for _ in range(PIPELINE_STREAMS)]
