@@ -395,6 +395,10 @@ def run_ours(args, rank, world, local_rank):
         acc.setdefault(name, []).append(v)
     phase_ms = {k: statistics.mean(v) for k, v in acc.items()}
 
+    # end to end through the host-buffer API: every rank takes part (at N > 1
+    # the steps' partial sums are gathered and combined inside the timed region)
+    e2e = measure_e2e(args, gm, sc, pts_d, world=world, dev=dev)
+
     if rank != 0:
         return
 
@@ -456,8 +460,8 @@ def run_ours(args, rank, world, local_rank):
     }
     line["clocks"] = clk.summary()
 
+    line["e2e"] = e2e
     if world == 1:
-        line["e2e"] = measure_e2e(args, gm, sc, pts_d)
         if not args.no_extra:
             line["extra"] = measure_extra(gm, wl, dev, imad_peak)
             pts_h = gm.to_numpy_points(pts_d[:CPU_SAMPLE], 1)
@@ -474,7 +478,7 @@ def run_ours(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
-def measure_e2e(args, gm, sc, pts_d):
+def measure_e2e(args, gm, sc, pts_d, world=1, dev=None):
     """End to end through the public host-buffer API, pinned host buffers:
     every step copies its points and scalars to the device, runs the MSM and
     reads its result back to the host.
@@ -482,7 +486,10 @@ def measure_e2e(args, gm, sc, pts_d):
     value: gm_g1_msm_host_async round-robin on PIPELINE_STREAMS streams, so
     that one step's copies overlap the previous steps' compute (each step's
     copies and result read are still inside the timed region).  sync_value: the blocking
-    g1_msm_limbs_wrapper, one MSM at a time."""
+    g1_msm_limbs_wrapper, one MSM at a time (one GPU only).  With N ranks each
+    rank runs the steps on its own shard; the steps' partial sums are then
+    gathered once and added on the device, inside the timed region, and the
+    time is the maximum over ranks."""
     import torch
     n = len(sc)
     pts_pin = torch.empty((n, gm.G1_WORDS), dtype=torch.int64, pin_memory=True)
@@ -499,10 +506,12 @@ def measure_e2e(args, gm, sc, pts_d):
 
     for _ in range(2):
         ref = gm.msm(pts_np, sc_np, group=1, montgomery=True)
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        gm.msm(pts_np, sc_np, group=1, montgomery=True)
-    sync_dt = (time.perf_counter() - t0) / steps
+    sync_dt = None
+    if world == 1:
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            gm.msm(pts_np, sc_np, group=1, montgomery=True)
+        sync_dt = (time.perf_counter() - t0) / steps
 
     ns = PIPELINE_STREAMS
     streams = [torch.cuda.Stream() for _ in range(ns)]
@@ -514,20 +523,50 @@ def measure_e2e(args, gm, sc, pts_d):
         gm.msm_host_async(pts_np, sc_np, res_np[i:i + 1], stream=streams[i], err=err_np[i:i + 1])
     for st in streams:
         st.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
     t0 = time.perf_counter()
     for i in range(ns, steps + ns):
         gm.msm_host_async(pts_np, sc_np, res_np[i:i + 1], stream=streams[i % ns], err=err_np[i:i + 1])
     for st in streams:
         st.synchronize()
-    dt = (time.perf_counter() - t0) / steps
+    if world > 1:
+        # every step's full MSM: its partial sums from all ranks, gathered
+        # once and added on the device, then read back
+        parts = torch.from_numpy(res_np[ns:].view(np.uint64).view(np.int64).reshape(-1).copy()).to(dev)
+        gathered = torch.empty(world * parts.numel(), dtype=torch.int64, device=dev)
+        dist.all_gather_into_tensor(gathered, parts)
+        g = gathered.view(world, steps, gm.G1P_WORDS)
+        full = torch.empty((steps, gm.G1P_WORDS), dtype=torch.int64, device=dev)
+        for k in range(steps):
+            gm.sum_projective(g[:, k, :].contiguous(), group=1, out=full[k])
+        full_h = full.cpu()
+    dt = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([dt], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dt = float(t.item())
+    dt /= steps
     want = gm.canonical_affine(ref.reshape(1), 1)
     ok = bool(err_np.max() == 0) and all(
         np.array_equal(gm.canonical_affine(res_np[i:i + 1], 1), want) for i in range(steps + ns))
-    return {"value": n / dt, "unit": "points/s", "h2d_bytes_per_step": n * (120 + 40),
-            "d2h_bytes_per_step": 168 + 4, "ms_per_step": dt * 1e3,
-            "api": f"gm_g1_msm_host_async on {ns} streams (host buffers, pinned)", "results_equal": ok,
-            "sync_value": n / sync_dt, "sync_ms_per_step": sync_dt * 1e3,
-            "sync_api": "g1_msm_limbs_wrapper (host buffers, pinned)"}
+    out = {"value": world * n / dt, "unit": "points/s", "h2d_bytes_per_step": n * (120 + 40),
+           "d2h_bytes_per_step": 168 + 4, "ms_per_step": dt * 1e3,
+           "api": f"gm_g1_msm_host_async on {ns} streams (host buffers, pinned)", "results_equal": ok}
+    if world > 1:
+        fh = full_h.numpy().view(np.uint64).view(gm.G1P).reshape(-1)
+        first = gm.canonical_affine(fh[:1], 1)
+        out["api"] += (f"; each rank its own shard, the {steps} steps' partial sums gathered once and added "
+                       "on the device inside the timed region, max over ranks")
+        out["results_equal"] = ok and all(np.array_equal(gm.canonical_affine(fh[k:k + 1], 1), first)
+                                          for k in range(steps))
+        out["h2d_bytes_per_step"] = world * n * (120 + 40)
+        out["d2h_bytes_per_step"] = world * (168 + 4) + 168
+    else:
+        out.update({"sync_value": n / sync_dt, "sync_ms_per_step": sync_dt * 1e3,
+                    "sync_api": "g1_msm_limbs_wrapper (host buffers, pinned)"})
+    return out
 
 
 def measure_fp2_micro(gm, wl, dev, imad_peak, reps=5, check_n=1 << 14):
